@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark of the plain FP64 GPU time step (cell-steps/s at 257^3).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the 257^3-node grid on [-1,1]^3 (h = 1/128, the "256^3"
+of the headline metric), Douglas-ADI + MIB-L2, torus R=0.5 r=0.2, beta 1:1000,
+exact solution e^{-t}(...) (eq 8), dt = h, plain FP64.  A "step" is one time
+step of that problem.  Each field is 136 MB and a step streams ~1 GB, larger
+than the 126 MB L2, so no explicit L2 flush is needed between steps.
+
+Multi-GPU: one independent replica per rank (the path does not shard; no
+collective on the data path), weak scaling; value = all ranks' cell-steps over
+the max-over-ranks device time.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "matched-time-splitting-3d_b200"))
+
+WORKLOAD = dict(n=(257, 257, 257), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, eq=8,
+                method="adi", mib=2, dt=2.0 / 256)
+METRIC = "cell-steps/s @256^3 plain FP64"
+
+# Algorithmic HBM bytes per grid node per launch of each kernel slot
+# (field reads/writes at 8 B plus the 1-byte node tag; scratch excluded).
+ALG_BYTES = {
+    "adi": {1: 17, 2: 17, 3: 25},
+    "lod-ie": {1: 17, 2: 17, 3: 17},
+    "lod-cn": {1: 17, 2: 17, 3: 17},
+    "ts": {1: 17, 2: 17, 3: 17, 4: 17, 5: 17},
+}
+SLOT_NAMES = {
+    "adi": ["jumps", "adi_x_sweep", "adi_y_sweep", "adi_z_sweep"],
+    "lod-ie": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
+    "lod-cn": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
+    "ts": ["jumps", "ts_explicit_x", "ts_explicit_y", "ts_z_sweep", "ts_y_sweep", "ts_x_sweep"],
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=257, help="nodes per axis")
+    ap.add_argument("--method", default="adi", choices=["adi", "lod-ie", "lod-cn", "ts"])
+    ap.add_argument("--surface", default="torus", choices=["torus", "ellipsoid"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: auto)")
+    return ap.parse_args()
+
+
+def workload(a):
+    w = dict(WORKLOAD)
+    w["n"] = (a.n, a.n, a.n)
+    w["dt"] = 2.0 / (a.n - 1)
+    w["method"] = a.method
+    if a.surface == "ellipsoid":
+        w["surface"] = "ellipsoid"
+        w["surface_params"] = (0.7001, 0.4999, 0.4001, 1.0, 0.0, 0.0, 0.0)
+    return w
+
+
+def config_of(w, world):
+    return {
+        "workload": f"{w['n'][0]}^3 {w['method']} MIB-L{w['mib']} {w['surface']}{tuple(w['surface_params'])} "
+                    f"beta {w['beta_in']}:{w['beta_out']} eq{w['eq']} dt=h plain FP64",
+        "grid": list(w["n"]),
+        "method": w["method"],
+        "mib": w["mib"],
+        "surface": w["surface"],
+        "surface_params": list(w["surface_params"]),
+        "beta": [w["beta_in"], w["beta_out"]],
+        "dt": w["dt"],
+        "replicas": world,
+        "parallelism": f"replicas x{world}",
+        "l2_flush": "not needed: inputs larger than L2 (136 MB per field, ~1 GB streamed per step)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for ln in f:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the reference's own code on the host cores
+
+def reference_binary():
+    for name in ("mts_ref_noaux", "mts_ref"):
+        p = os.path.join(ROOT, "oracle", "_ref", name)
+        if os.path.exists(p):
+            return p
+    return None
+
+
+def mem_available_gb() -> float:
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 16.0
+
+
+def run_reference_sample(w, procs: int, steps_per_proc: int, timeout: float = 900):
+    """Runs `procs` independent copies of the reference binary on the
+    workload, each for `steps_per_proc` time steps, concurrently on the host
+    cores.  Returns (cell-steps/s, cores, sample text, kind) from the binaries'
+    own step timers (setup excluded)."""
+    binary = reference_binary()
+    n = w["n"]
+    sp = list(w["surface_params"])
+    if binary is None:
+        return None
+    args = [binary, "--n", *map(str, n), "--surface", w["surface"], *map(repr, sp), "--beta", repr(w["beta_in"]),
+            repr(w["beta_out"]), "--eq", str(w["eq"]), "--method", w["method"], "--mib", str(w["mib"]), "--dt",
+            repr(w["dt"]), "--steps", str(steps_per_proc)]
+    ps = [subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for _ in range(procs)]
+    secs = []
+    for p in ps:
+        out, _ = p.communicate(timeout=timeout)
+        line = [ln for ln in out.splitlines() if ln.startswith("{")]
+        if not line:
+            raise RuntimeError("reference run produced no result line")
+        secs.append(json.loads(line[-1])["step_seconds"])
+    nodes = n[0] * n[1] * n[2]
+    value = procs * nodes * steps_per_proc / max(secs)
+    sample = (f"{procs} concurrent single-threaded reference processes ({os.path.basename(binary)}), each "
+              f"{steps_per_proc} step(s) of the {n[0]}^3 workload; per-process step time "
+              f"{min(secs):.2f}-{max(secs):.2f} s (setup excluded)")
+    return value, procs, sample, "reference"
+
+
+def auto_procs(w) -> int:
+    nodes = w["n"][0] * w["n"][1] * w["n"][2]
+    per_proc_gb = 1.5 * nodes / 257 ** 3 + 0.05
+    cores = os.cpu_count() or 1
+    return max(1, min(cores, 16, int(mem_available_gb() * 0.6 / per_proc_gb)))
+
+
+# ---------------------------------------------------------------------------
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_setup()
+    w = workload(a)
+    nodes = w["n"][0] * w["n"][1] * w["n"][2]
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = a.ref_procs or auto_procs(w)
+        res = run_reference_sample(w, procs, 1)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+            return 0
+        value, cores, sample, kind = res
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": a.gpus,
+            "steps": procs, "warmup": 0, "ms_per_step": 1e3 * nodes / value * procs / procs,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic exact solution)", "config": config_of(w, 1),
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import mts_b200 as M
+
+    spec = M.Spec(**w)
+    solver = M.Solver(spec)
+    solver.initialize()
+    solver.advance(a.warmup)
+    solver.synchronize()
+
+    stream = torch.cuda.ExternalStream(solver.stream())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(torch.cuda.current_device())
+    launches0 = solver.launch_count()
+    solver.set_profiling(True)
+    solver.profile_read()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0.record(stream)
+    solver.advance(a.steps)
+    ev1.record(stream)
+    solver.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    kms, kn = solver.profile_read()
+    solver.set_profiling(False)
+    launches = solver.launch_count() - launches0
+    lmax, l2, _ = solver.norms()
+
+    # end to end through the C ABI with host buffers: the field goes up and
+    # comes back every step (the reference's Solve_2nd contract on a host
+    # CubicDoub), pinned host memory.
+    e2e_steps = max(1, a.e2e_steps)
+    hu = torch.empty(nodes, dtype=torch.float64, pin_memory=True)
+    hu.copy_(torch.from_numpy(solver.solution()))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    solver.advance_host_ptr(hu.data_ptr(), hu.data_ptr(), 1)
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        solver.advance_host_ptr(hu.data_ptr(), hu.data_ptr(), 1)
+    e1.record(stream)
+    solver.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+
+    t_all = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
+    ms_max, e2e_max = float(t_all[0]), float(t_all[1])
+    value = world * nodes * a.steps / (ms_max / 1e3)
+    e2e_value = world * nodes * e2e_steps / (e2e_max / 1e3)
+
+    method = w["method"]
+    names = SLOT_NAMES[method]
+    kernels = {}
+    for k, name in enumerate(names):
+        if kn[k] > 0:
+            kernels[name] = {"ms_per_launch": kms[k] / kn[k], "launches": int(kn[k]),
+                             "share": kms[k] / max(1e-12, kms[: len(names)].sum())}
+    dom = max((k for k in ALG_BYTES[method]), key=lambda k: kms[k])
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    per_launch_ms = kms[dom] / kn[dom]
+    achieved = ALG_BYTES[method][dom] * nodes / (per_launch_ms / 1e3) / 1e9
+    step_bytes = sum(ALG_BYTES[method].values())
+    roofline = {
+        "bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})",
+        "traffic": None,
+        "algorithmic_bytes_per_node": ALG_BYTES[method][dom],
+        "step": {"bytes_per_node_step": step_bytes,
+                 "achieved": step_bytes * nodes * a.steps / (ms / 1e3) / 1e9,
+                 "frac": step_bytes * nodes * a.steps / (ms / 1e3) / 1e9 / peak},
+    }
+    traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_path):
+        with open(traffic_path) as f:
+            tr = json.load(f).get(f"{method}:{names[dom]}")
+        if tr:
+            roofline["traffic"] = tr["bytes_per_node"] * nodes
+            roofline["traffic_source"] = tr["source"]
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic exact solution, seeded geometry)",
+        "config": config_of(w, world), "gpu_launches": int(launches), "kernels": kernels, "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * nodes,
+                "d2h_bytes_per_step": 8 * nodes, "steps": e2e_steps,
+                "api": "mts_advance_host (field uploaded and downloaded every step, pinned host memory)"},
+        "clocks": clk, "accuracy": {"lmax": lmax, "l2": l2, "t": solver.time},
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            res = run_reference_sample(w, a.ref_procs or auto_procs(w), 1)
+        except Exception as e:  # the baseline is reported, never required
+            res = None
+            line["cpu_baseline_error"] = str(e)[:200]
+        if res is not None:
+            v, cores, sample, kind = res
+            line["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": kind,
+                                    "sample": sample}
+    solver.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,183 @@
+/* Matched-TS on B200: C ABI of the GPU time-stepping path.
+ *
+ * One handle = one parabolic interface problem resident on one GPU: grid,
+ * node tags, the MIB crossing list with its fictitious-point weights, the
+ * time-invariant line-solve coefficients and the solution field stay in
+ * device memory for all time steps; per step only the time crosses the bus.
+ *
+ * Fields are float64, x fastest: index = ix + nx*(iy + ny*iz), the order of
+ * Mesh::To1d in the reference (src/mesh/mesh.cc:93-99).  Every function
+ * returns an mts_status; no function exits or throws.  Functions on one
+ * handle are not thread-safe; distinct handles are independent (one CUDA
+ * stream each).
+ */
+#ifndef MTS_H
+#define MTS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MTS_OK = 0,
+  MTS_ERR_ARG = 1,           /* bad argument or unsupported option */
+  MTS_ERR_SETUP = 2,         /* reference setup abort: interface on a grid node,
+                                coherent corners, open surface, singular LU */
+  MTS_ERR_ZERO_PIVOT = 3,    /* zero pivot in a line solve (TDMA "tridag" throw) */
+  MTS_ERR_NONFINITE = 4,     /* root finding failed to bracket / converge */
+  MTS_ERR_CUDA = 5,          /* CUDA runtime error (see mts_last_error) */
+  MTS_ERR_NO_DEVICE = 6,     /* no CUDA device visible */
+  MTS_ERR_OOM = 7            /* device allocation failed */
+} mts_status;
+
+typedef enum { MTS_ADI = 0, MTS_LOD_IE = 1, MTS_LOD_CN = 2, MTS_TS = 3 } mts_method;
+typedef enum { MTS_SURFACE_ELLIPSOID = 0, MTS_SURFACE_TORUS = 1 } mts_surface_kind;
+
+/* Uniform grid on [xl,xr]x[yl,yr]x[zl,zr] with nx*ny*nz nodes (Mesh ctor,
+ * src/mesh/mesh.h:20). */
+typedef struct {
+  int32_t nx, ny, nz;
+  int32_t pad;
+  double xl, xr, yl, yr, zl, zr;
+} mts_grid;
+
+/* Level set.  Ellipsoid: params = {a, b, c, r, cx, cy, cz} for
+ * (x-cx)^2/a^2 + (y-cy)^2/b^2 + (z-cz)^2/c^2 - r^2 (Surface_Ellipsoid,
+ * src/surface/surface_ellipsoid.h with a centre); torus: params = {R, r} for
+ * (R - sqrt(x^2+y^2))^2 + z^2 - r^2 (Surface_Torus, src/surface/surface_torus.h). */
+typedef struct {
+  int32_t kind;
+  int32_t pad;
+  double params[7];
+} mts_surface;
+
+/* Problem parameters.  beta is piecewise constant (beta_in inside, beta_out
+ * outside).  eq selects the exact solution that supplies source, boundary and
+ * jump data: 0 = the reference's Eq_0 (src/equation/eq_0.cc), 8 = inside
+ * e^{-t} sin2x cos2y sin2z / outside e^{-t}(x^2+y^2+z^2).  mib is 1 (MIB-L1)
+ * or 2 (MIB-L2) as in Intersections(..., mib_method, ...). */
+typedef struct {
+  double beta_in, beta_out;
+  int32_t eq;
+  int32_t method; /* mts_method */
+  int32_t mib;
+  int32_t pad;
+  double dt;
+  double t0;
+} mts_params;
+
+/* One interface crossing, field by field the reference's Intersection_Data
+ * (src/constant.h:141-156): dir 0/1/2 = x/y/z; (indx1, indx2) = the grid
+ * line (x: iy,iz; y: ix,iz; z: ix,iy); id = ID (>0 irregular, <0 corner pair);
+ * left_loc; nwei = length of wei.weil[0]/weir[0]; p = local frame, row major. */
+typedef struct {
+  int32_t dir, indx1, indx2, id, left_loc, nwei;
+  double coord[3], gamma, normal[3], p[9], weil[9], weir[9];
+} mts_crossing;
+
+typedef struct mts_problem* mts_handle;
+
+/* Builds the mesh tags, crossing list and MIB weights on the host and
+ * uploads the problem to the current CUDA device.  Replaces the setup of
+ *   Mesh::Mesh            src/mesh/mesh.cc:20-70
+ *   Intersections ctor    src/spatial/intersection.cc:22-51 (crossings,
+ *                         MIB-L1/L2 weights via LU, src/decomposition/lu.cc)
+ * and the constructors Douglas_ADI / LOD / TS (src/temporal/douglas_adi.h:47,
+ * lod.h:51, trapezoidal.h:48).  The time starts at params->t0. */
+mts_status mts_create(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
+                      mts_handle* out);
+
+/* Same, from a caller-supplied mesh and crossing list (the drop-in path: the
+ * reference's Mesh::mesh_value and Intersections::ifpx/ifpy/ifpz, flattened).
+ * tags: nx*ny*nz values in {+1, -1}, x fastest. */
+mts_status mts_create_from_crossings(const mts_grid* grid, const int8_t* tags,
+                                     const mts_crossing* crossings, int32_t ncrossings,
+                                     const mts_params* params, mts_handle* out);
+
+mts_status mts_destroy(mts_handle h);
+
+/* The host half of mts_create alone (no device needed): node tags and the
+ * crossing list with MIB weights.  tags may be NULL; when out is NULL or
+ * capacity < *count only *count is set.  counts (may be NULL) receives
+ * [corner pairs, singular-matrix warnings]. */
+mts_status mts_setup_host(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
+                          int8_t* tags, mts_crossing* out, int32_t capacity, int32_t* count,
+                          int64_t counts[2]);
+
+/* Initialization (douglas_adi.cc:1684-1714, lod/trapezoidal copies): the
+ * exact solution at the current time, by node tag, written on the device. */
+mts_status mts_initialize(mts_handle h);
+
+/* Host <-> device copies of the solution field (nx*ny*nz doubles). */
+mts_status mts_set_solution(mts_handle h, const double* u);
+mts_status mts_get_solution(mts_handle h, double* u);
+
+/* One step of the handle's method ending at t_next.  Replaces
+ *   Douglas_ADI::Solve_2nd(eq(t_next), inter, uh, beta)   douglas_adi.cc:66-1110
+ *   LOD::Solve_2nd(eq(t_next), inter, uh, beta, 'I'|'C')   lod.cc:44-205
+ *   TS::Solve_2nd(eq(t_prev), eq(t_half), eq(t_next), ...)  trapezoidal.cc:46-272
+ * t_prev and t_half are read by TS only.  Refresh_Jump (intersection.cc:
+ * 2294-2490) runs on the device inside the step.  Asynchronous. */
+mts_status mts_solve_2nd(mts_handle h, double t_prev, double t_half, double t_next);
+
+/* nsteps steps of the time loop of src/helper.h:199-238 (t += dt before each
+ * step; TS evaluates at t-dt, t-dt/2, t).  Asynchronous. */
+mts_status mts_advance(mts_handle h, int32_t nsteps);
+
+/* The same loop with the caller's host field: u_in is uploaded, nsteps steps
+ * run, the result is downloaded into u_out (which may equal u_in).  This is
+ * the per-call cost of the reference's Solve_2nd(..., CubicDoub& uh, ...)
+ * contract with the field in host memory. */
+mts_status mts_advance_host(mts_handle h, const double* u_in, double* u_out, int32_t nsteps);
+
+/* Error (douglas_adi.cc:1723-1770): L-infinity with its first argmax in
+ * [ix][iy][iz] loop order, and L2 = sqrt(sum e^2 / (nx ny nz)), against the
+ * exact solution at the current time.  Synchronous. */
+mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3);
+
+mts_status mts_get_time(mts_handle h, double* t);
+mts_status mts_set_time(mts_handle h, double t);
+
+/* Blocks until all work queued on the handle's stream is done; reports a
+ * zero pivot met by any line solve since the last check. */
+mts_status mts_synchronize(mts_handle h);
+
+/* Counts: [0..2] crossings per direction, [3..5] MIB row blocks per
+ * direction, [6] corner pairs, [7] singular-matrix warnings of the weight
+ * solves (intersection.cc:1034-1057 prints these and carries on). */
+mts_status mts_get_counts(mts_handle h, int64_t counts[8]);
+
+/* Host copies of the setup products (for parity checks): node tags (+1/-1,
+ * x fastest) and the crossing list in the reference's order (per direction
+ * x, y, z; lines in loop order; crossings by left_loc). */
+mts_status mts_export_tags(mts_handle h, int8_t* tags);
+mts_status mts_export_crossings(mts_handle h, mts_crossing* out, int32_t capacity, int32_t* count);
+
+/* Number of kernel launches the library has queued on this handle. */
+mts_status mts_get_launch_count(mts_handle h, int64_t* launches);
+
+/* The CUDA stream of the handle (a cudaStream_t), for callers that order
+ * their own work against it. */
+mts_status mts_get_stream(mts_handle h, void** stream);
+
+/* Per-kernel timing with CUDA events recorded on the handle's stream around
+ * every launch of a step (negligible overhead; off by default).  Slots, in
+ * launch order: Douglas-ADI and LOD {0 jumps, 1 x sweep, 2 y sweep, 3 z sweep};
+ * TS {0 jumps, 1 explicit x, 2 explicit y, 3 z sweep, 4 y sweep, 5 x sweep}.
+ * mts_profile_read synchronizes, returns the summed milliseconds and launch
+ * counts per slot since the last read, and resets them. */
+mts_status mts_set_profiling(mts_handle h, int32_t on);
+mts_status mts_profile_read(mts_handle h, double ms[8], int64_t launches[8]);
+
+/* Text of the last error on this thread. */
+const char* mts_last_error(void);
+
+/* ABI version (major*100 + minor). */
+int32_t mts_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MTS_H */

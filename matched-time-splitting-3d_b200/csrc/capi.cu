@@ -1,0 +1,648 @@
+// C ABI of the GPU path (include/mts.h): handle lifecycle, the one-time
+// precompute of the time-invariant MIB row blocks, device residency, and the
+// per-step launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mts.h"
+#include "device.h"
+#include "setup.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+mts_status fail(mts_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+#define CUDA_TRY(call)                                                             \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      return fail(e_ == cudaErrorMemoryAllocation ? MTS_ERR_OOM : MTS_ERR_CUDA,    \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    }                                                                              \
+  } while (0)
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t n, cudaStream_t st) {
+  *dst = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
+  if (e != cudaSuccess) return e;
+  if (src) return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st);
+  return cudaSuccess;
+}
+
+}  // namespace
+
+struct mts_problem {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  mts::Grid g;
+  mts_params prm{};
+  std::vector<int8_t> tags;
+  std::vector<mts_crossing> cross;
+  mts::SetupReport rep;
+  int64_t nblk[3] = {0, 0, 0};
+  int64_t ncr[3] = {0, 0, 0};
+  mts::Dev dev{};
+  double* u0 = nullptr;
+  double* u1 = nullptr;
+  std::vector<void*> allocations;
+  double* norm_part = nullptr;
+  double* norm_out = nullptr;
+  double* host_norm = nullptr;  // pinned, 3 doubles
+  int norm_nb = 1;
+  double t = 0;
+  int64_t launches = 0;
+  // per-kernel event timing (mts_set_profiling)
+  bool profiling = false;
+  std::vector<std::array<cudaEvent_t, 2 * mts::kProfileSlots>> ev_busy, ev_free;
+  double prof_ms[mts::kProfileSlots] = {};
+  int64_t prof_n[mts::kProfileSlots] = {};
+
+  int slots() const { return prm.method == MTS_TS ? 6 : 4; }
+
+  ~mts_problem() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& a : ev_busy)
+      for (cudaEvent_t e : a) cudaEventDestroy(e);
+    for (auto& a : ev_free)
+      for (cudaEvent_t e : a) cudaEventDestroy(e);
+    for (void* p : allocations) cudaFree(p);
+    if (host_norm) cudaFreeHost(host_norm);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  template <class T>
+  cudaError_t put(T** dst, const T* src, size_t n) {
+    cudaError_t e = upload(dst, src, n, stream);
+    if (*dst) allocations.push_back((void*)*dst);
+    return e;
+  }
+};
+
+namespace {
+
+// Convert2Tri_irr / _cor (src/temporal/douglas_adi.cc:1554-1577, 1637-1675)
+// applied to the matrix part of a MIB row block, once: the coefficients do
+// not change between steps.  The multipliers are kept so that each step
+// replays the same row operations on its right-hand side.
+void precompute_block(mts::MibBlock& b, double cdt, const double vd[3][3]) {
+  if (b.kind == 2) {
+    double row[2][4];
+    std::memset(row, 0, sizeof row);
+    row[0][0] = -cdt * vd[0][0];
+    row[0][1] = 1 - cdt * vd[0][1];
+    for (int i = 0; i < 4; i++) row[0][i] += -cdt * vd[0][2] * b.w[1][i];
+    row[1][2] = 1 - cdt * vd[1][1];
+    row[1][3] = -cdt * vd[1][2];
+    for (int i = 0; i < 4; i++) row[1][i] += -cdt * vd[1][0] * b.w[0][i];
+    double rate = row[1][0] / row[0][0];
+    for (int i = 0; i < 4; i++) row[1][i] -= rate * row[0][i];
+    b.rate[0] = rate;
+    rate = row[0][3] / row[1][3];
+    for (int i = 0; i < 4; i++) row[0][i] -= rate * row[1][i];
+    b.rate[1] = rate;
+    for (int i = 0; i < 2; i++) {
+      b.ia[i] = row[i][i];
+      b.ib[i] = row[i][i + 1];
+      b.ic[i] = row[i][i + 2];
+    }
+  } else {
+    double row[3][5];
+    std::memset(row, 0, sizeof row);
+    row[0][0] = -cdt * vd[0][0];
+    row[0][1] = 1 - cdt * vd[0][1];
+    for (int i = 0; i < 5; i++) row[0][i] -= cdt * vd[0][2] * b.w[1][i];
+    row[1][2] = 1 - cdt * vd[1][1];
+    for (int i = 0; i < 5; i++) row[1][i] -= cdt * vd[1][0] * b.w[0][i];
+    for (int i = 0; i < 5; i++) row[1][i] -= cdt * vd[1][2] * b.w[3][i];
+    row[2][3] = 1 - cdt * vd[2][1];
+    row[2][4] = -cdt * vd[2][2];
+    for (int i = 0; i < 5; i++) row[2][i] -= cdt * vd[2][0] * b.w[2][i];
+    double r1 = row[1][0] / row[0][0], r2 = row[2][0] / row[0][0];
+    for (int i = 0; i < 5; i++) {
+      row[1][i] -= r1 * row[0][i];
+      row[2][i] -= r2 * row[0][i];
+    }
+    double r0b = row[0][4] / row[2][4], r1b = row[1][4] / row[2][4];
+    for (int i = 0; i < 5; i++) {
+      row[0][i] -= r0b * row[2][i];
+      row[1][i] -= r1b * row[2][i];
+    }
+    double r2b = row[2][1] / row[1][1];
+    for (int i = 0; i < 5; i++) row[2][i] -= r2b * row[1][i];
+    double r0c = row[0][3] / row[1][3];
+    for (int i = 0; i < 5; i++) row[0][i] -= r0c * row[1][i];
+    b.rate[0] = r1;
+    b.rate[1] = r2;
+    b.rate[2] = r0b;
+    b.rate[3] = r1b;
+    b.rate[4] = r2b;
+    b.rate[5] = r0c;
+    for (int i = 0; i < 3; i++) {
+      b.ia[i] = row[i][i];
+      b.ib[i] = row[i][i + 1];
+      b.ic[i] = row[i][i + 2];
+    }
+  }
+}
+
+int line_count(const mts::Grid& g, int d) {
+  int n1 = d == 0 ? g.ny : g.nx;
+  int n2 = d == 2 ? g.ny : g.nz;
+  return n1 * n2;
+}
+
+// Builds every device-side table of a problem from its grid, tags and
+// crossing list, and uploads them.
+mts_status finish_create(mts_problem* h) {
+  const mts::Grid& g = h->g;
+  const mts_params& p = h->prm;
+  const long long N = g.nodes();
+  mts::Dev& D = h->dev;
+  D.nx = g.nx;
+  D.ny = g.ny;
+  D.nz = g.nz;
+  D.nn = N;
+  D.eq = p.eq;
+  D.method = p.method;
+  D.dt = p.dt;
+  D.kex = 0.5 * p.dt;
+  const double coef = (p.method == MTS_LOD_CN || p.method == MTS_TS) ? 0.5 : 1;
+  D.cdt = coef * p.dt;
+  D.hdt = 0.5 * p.dt;
+  D.bi = p.beta_in;
+  D.bo = p.beta_out;
+  D.kin = 12.0 * p.beta_in - 1.0;
+  D.c6bo = 6.0 * p.beta_out;
+  const double h3[3] = {g.dx, g.dy, g.dz};
+  for (int d = 0; d < 3; d++)
+    for (int side = 0; side < 2; side++) {
+      double beta = side ? p.beta_out : p.beta_in;
+      double hh = h3[d];
+      D.vd[d][side][0] = beta / (hh * hh);
+      D.vd[d][side][1] = -(beta + beta) / (hh * hh);
+      D.vd[d][side][2] = beta / (hh * hh);
+      D.ia[d][side] = -D.cdt * D.vd[d][side][0];
+      D.ib[d][side] = 1 - D.cdt * D.vd[d][side][1];
+      D.ic[d][side] = -D.cdt * D.vd[d][side][2];
+    }
+
+  // node tags with MIB-row flags; blocks per direction
+  std::vector<uint8_t> tag8((size_t)N);
+  for (long long m = 0; m < N; m++) tag8[m] = h->tags[m] == 1 ? mts::TAG_OUT : 0;
+  std::vector<mts::MibBlock> blocks[3];
+  std::vector<int32_t> bstart[3];
+  std::vector<mts::CrossConst> cc(h->cross.size());
+  // order crossings per direction by (line, left_loc), keeping pairs together
+  std::vector<int> order(h->cross.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+  auto lid = [&](const mts_crossing& c) {
+    int n2 = c.dir == 2 ? g.ny : g.nz;
+    return (long long)c.indx1 * n2 + c.indx2;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const mts_crossing &A = h->cross[a], &B = h->cross[b];
+    if (A.dir != B.dir) return A.dir < B.dir;
+    long long la = lid(A), lb = lid(B);
+    if (la != lb) return la < lb;
+    return A.left_loc < B.left_loc;
+  });
+  for (int d = 0; d < 3; d++) bstart[d].assign((size_t)line_count(g, d) + 1, 0);
+  const uint8_t flag[3] = {mts::TAG_MIBX, mts::TAG_MIBY, mts::TAG_MIBZ};
+  for (size_t k = 0; k < order.size();) {
+    const int ci = order[k];
+    const mts_crossing& c = h->cross[ci];
+    if (c.dir < 0 || c.dir > 2) return fail(MTS_ERR_ARG, "crossing direction out of range");
+    const int d = c.dir;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+    if (c.indx1 < 1 || c.indx1 >= n[a1] - 1 || c.indx2 < 1 || c.indx2 >= n[a2] - 1 || c.left_loc < 1)
+      return fail(MTS_ERR_ARG, "crossing outside the interior lines");
+    mts::MibBlock b;
+    std::memset(&b, 0, sizeof b);
+    b.line = (int32_t)lid(c);
+    b.L = c.left_loc;
+    b.c0 = ci;
+    if (c.id > 0) {
+      b.kind = 2;
+      b.c1 = ci;
+      std::memcpy(b.w[0], c.weil, sizeof c.weil);
+      std::memcpy(b.w[1], c.weir, sizeof c.weir);
+      k += 1;
+    } else {
+      if (k + 1 >= order.size()) return fail(MTS_ERR_ARG, "corner crossing without its pair");
+      const int cj = order[k + 1];
+      const mts_crossing& r = h->cross[cj];
+      if (r.id >= 0 || r.dir != d || lid(r) != lid(c) || r.left_loc != c.left_loc + 1)
+        return fail(MTS_ERR_ARG, "corner crossing without its pair");
+      b.kind = 3;
+      b.c1 = cj;
+      std::memcpy(b.w[0], c.weil, sizeof c.weil);
+      std::memcpy(b.w[1], c.weir, sizeof c.weir);
+      std::memcpy(b.w[2], r.weil, sizeof r.weil);
+      std::memcpy(b.w[3], r.weir, sizeof r.weir);
+      k += 2;
+    }
+    // the fictitious-point stencils read nodes L-1 .. L+kind: all must exist
+    if (b.L + b.kind >= n[d]) return fail(MTS_ERR_ARG, "crossing block runs past the line end");
+    if (!blocks[d].empty() && blocks[d].back().line == b.line && blocks[d].back().L + blocks[d].back().kind > b.L)
+      return fail(MTS_ERR_ARG, "overlapping crossing blocks on one line");
+    double vdr[3][3];
+    for (int q = 0; q < b.kind; q++) {
+      int idx3[3];
+      idx3[a1] = c.indx1;
+      idx3[a2] = c.indx2;
+      idx3[d] = b.L + q;
+      long long m = g.index(idx3[0], idx3[1], idx3[2]);
+      int side = h->tags[m] == 1;
+      for (int z = 0; z < 3; z++) vdr[q][z] = D.vd[d][side][z];
+      tag8[m] |= flag[d];
+    }
+    precompute_block(b, D.cdt, vdr);
+    blocks[d].push_back(b);
+    bstart[d][b.line + 1]++;
+  }
+  for (int d = 0; d < 3; d++) {
+    for (size_t l = 0; l + 1 < bstart[d].size(); l++) bstart[d][l + 1] += bstart[d][l];
+    h->nblk[d] = (int64_t)blocks[d].size();
+  }
+  for (size_t i = 0; i < h->cross.size(); i++) {
+    const mts_crossing& c = h->cross[i];
+    mts::CrossConst& q = cc[i];
+    q.x = c.coord[0];
+    q.y = c.coord[1];
+    q.z = c.coord[2];
+    q.R2 = (q.x * q.x + q.y * q.y) + q.z * q.z;
+    q.S = (std::sin(2.0 * q.x) * std::cos(2.0 * q.y)) * std::sin(2.0 * q.z);
+    q.D[0] = ((2.0 * std::cos(2.0 * q.x)) * std::cos(2.0 * q.y)) * std::sin(2.0 * q.z);
+    q.D[1] = ((-2.0 * std::sin(2.0 * q.x)) * std::sin(2.0 * q.y)) * std::sin(2.0 * q.z);
+    q.D[2] = ((2.0 * std::sin(2.0 * q.x)) * std::cos(2.0 * q.y)) * std::cos(2.0 * q.z);
+    for (int k = 0; k < 3; k++) q.p[k] = c.p[k];
+    if (!mts::frame_inverse_col0(c.p, c.dir, &q.pinv)) return fail(MTS_ERR_SETUP, "singular local frame");
+    h->ncr[c.dir]++;
+  }
+  D.ncross = (int)h->cross.size();
+
+  // axis tables
+  std::vector<double> axv[3], s2v[3], c2v[3];
+  const std::vector<double>* axes[3] = {&g.x, &g.y, &g.z};
+  for (int d = 0; d < 3; d++) {
+    axv[d] = *axes[d];
+    s2v[d].resize(axv[d].size());
+    c2v[d].resize(axv[d].size());
+    for (size_t i = 0; i < axv[d].size(); i++) {
+      s2v[d][i] = std::sin(2.0 * axv[d][i]);
+      c2v[d][i] = std::cos(2.0 * axv[d][i]);
+    }
+  }
+
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CUDA_TRY(h->put(&h->u0, (const double*)nullptr, (size_t)N));
+  CUDA_TRY(h->put(&h->u1, (const double*)nullptr, (size_t)N));
+  CUDA_TRY(h->put(&D.gam, (const double*)nullptr, (size_t)N));
+  if (p.method == MTS_ADI) {
+    CUDA_TRY(h->put(&D.ydt, (const double*)nullptr, (size_t)N));
+  }
+  uint8_t* dtag = nullptr;
+  CUDA_TRY(h->put(&dtag, tag8.data(), tag8.size()));
+  D.tag = dtag;
+  for (int d = 0; d < 3; d++) {
+    double *a = nullptr, *s = nullptr, *c = nullptr;
+    CUDA_TRY(h->put(&a, axv[d].data(), axv[d].size()));
+    CUDA_TRY(h->put(&s, s2v[d].data(), s2v[d].size()));
+    CUDA_TRY(h->put(&c, c2v[d].data(), c2v[d].size()));
+    D.ax[d] = a;
+    D.s2[d] = s;
+    D.c2[d] = c;
+    int32_t* bs = nullptr;
+    mts::MibBlock* bl = nullptr;
+    CUDA_TRY(h->put(&bs, bstart[d].data(), bstart[d].size()));
+    CUDA_TRY(h->put(&bl, blocks[d].empty() ? nullptr : blocks[d].data(), blocks[d].size()));
+    D.bstart[d] = bs;
+    D.blk[d] = bl;
+  }
+  mts::CrossConst* dcc = nullptr;
+  CUDA_TRY(h->put(&dcc, cc.empty() ? nullptr : cc.data(), cc.size()));
+  D.cc = dcc;
+  CUDA_TRY(h->put(&D.jv, (const double2*)nullptr, h->cross.size()));
+  CUDA_TRY(h->put(&D.status, (const int*)nullptr, 1));
+  CUDA_TRY(cudaMemsetAsync(D.status, 0, sizeof(int), h->stream));
+  h->norm_nb = mts::norms_blocks(D);
+  CUDA_TRY(h->put(&h->norm_part, (const double*)nullptr, (size_t)3 * h->norm_nb));
+  CUDA_TRY(h->put(&h->norm_out, (const double*)nullptr, 3));
+  CUDA_TRY(cudaMallocHost((void**)&h->host_norm, 3 * sizeof(double)));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->t = p.t0;
+  return MTS_OK;
+}
+
+mts_status check_params(const mts_grid* grid, const mts_params* p) {
+  if (!grid || !p) return fail(MTS_ERR_ARG, "null argument");
+  if (grid->nx < 3 || grid->ny < 3 || grid->nz < 3) return fail(MTS_ERR_ARG, "grid needs at least 3 nodes per axis");
+  if ((long long)grid->nx * grid->ny * grid->nz > (1LL << 40)) return fail(MTS_ERR_ARG, "grid too large");
+  if (!(grid->xr > grid->xl) || !(grid->yr > grid->yl) || !(grid->zr > grid->zl))
+    return fail(MTS_ERR_ARG, "empty domain");
+  if (p->eq != 0 && p->eq != 8) return fail(MTS_ERR_ARG, "eq must be 0 or 8");
+  if (p->method < MTS_ADI || p->method > MTS_TS) return fail(MTS_ERR_ARG, "unknown method");
+  if (p->mib != 1 && p->mib != 2) return fail(MTS_ERR_ARG, "mib must be 1 or 2");
+  if (!(p->dt > 0)) return fail(MTS_ERR_ARG, "dt must be positive");
+  if (!(p->beta_in > 0) || !(p->beta_out > 0)) return fail(MTS_ERR_ARG, "beta must be positive");
+  return MTS_OK;
+}
+
+mts_status check_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(MTS_ERR_NO_DEVICE, "no CUDA device visible");
+  return MTS_OK;
+}
+
+mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_next) {
+  mts::StepTimes T;
+  T.e_prev = std::exp(-t_prev);
+  T.e_half = std::exp(-t_half);
+  T.e_next = std::exp(-t_next);
+  cudaEvent_t* ev = nullptr;
+  if (h->profiling) {
+    if (h->ev_free.empty()) {
+      std::array<cudaEvent_t, 2 * mts::kProfileSlots> a;
+      for (auto& e : a) {
+        cudaError_t ce = cudaEventCreate(&e);
+        if (ce != cudaSuccess) return fail(MTS_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(ce));
+      }
+      h->ev_free.push_back(a);
+    }
+    h->ev_busy.push_back(h->ev_free.back());
+    h->ev_free.pop_back();
+    ev = h->ev_busy.back().data();
+  }
+  h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(MTS_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+  h->t = t_next;
+  return MTS_OK;
+}
+
+mts_status advance(mts_problem* h, int nsteps) {
+  const double dt = h->prm.dt;
+  for (int s = 0; s < nsteps; s++) {
+    double t1 = h->t + dt;
+    mts_status st = enqueue_step(h, t1 - dt, t1 - 0.5 * dt, t1);
+    if (st) return st;
+  }
+  return MTS_OK;
+}
+
+mts_status sync_status(mts_problem* h) {
+  int flag = 0;
+  CUDA_TRY(cudaMemcpyAsync(&flag, h->dev.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (flag & 1) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line solve");
+  return MTS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t mts_version(void) { return 100; }
+
+const char* mts_last_error(void) { return g_last_error.c_str(); }
+
+mts_status mts_create(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
+                      mts_handle* out) {
+  if (!out || !surface) return fail(MTS_ERR_ARG, "null argument");
+  *out = nullptr;
+  mts_status st = check_params(grid, params);
+  if (st) return st;
+  st = check_device();
+  if (st) return st;
+  std::unique_ptr<mts::Surface> surf(mts::make_surface(*surface));
+  if (!surf) return fail(MTS_ERR_ARG, "unknown surface kind");
+  std::unique_ptr<mts_problem> h(new mts_problem());
+  cudaGetDevice(&h->device);
+  h->g = mts::make_grid(*grid);
+  h->prm = *params;
+  st = mts::build_tags(h->g, *surf, h->tags);
+  if (st) return fail(st, "a grid node lies on the interface");
+  st = mts::build_crossings(h->g, h->tags, *surf, params->beta_in, params->beta_out, params->mib, h->cross, &h->rep);
+  if (st) return fail(st, "interface setup failed (root finding, coherent corners, open surface or singular LU)");
+  st = finish_create(h.get());
+  if (st) return st;
+  *out = h.release();
+  return MTS_OK;
+}
+
+mts_status mts_create_from_crossings(const mts_grid* grid, const int8_t* tags, const mts_crossing* crossings,
+                                     int32_t ncrossings, const mts_params* params, mts_handle* out) {
+  if (!out || !tags || (ncrossings > 0 && !crossings) || ncrossings < 0) return fail(MTS_ERR_ARG, "null argument");
+  *out = nullptr;
+  mts_status st = check_params(grid, params);
+  if (st) return st;
+  st = check_device();
+  if (st) return st;
+  std::unique_ptr<mts_problem> h(new mts_problem());
+  cudaGetDevice(&h->device);
+  h->g = mts::make_grid(*grid);
+  h->prm = *params;
+  h->tags.assign(tags, tags + h->g.nodes());
+  for (int8_t v : h->tags)
+    if (v != 1 && v != -1) return fail(MTS_ERR_ARG, "tags must be +1 or -1");
+  h->cross.assign(crossings, crossings + ncrossings);
+  for (const mts_crossing& c : h->cross) h->rep.corner_pairs += c.id < 0;
+  h->rep.corner_pairs /= 2;
+  st = finish_create(h.get());
+  if (st) return st;
+  *out = h.release();
+  return MTS_OK;
+}
+
+mts_status mts_setup_host(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
+                          int8_t* tags, mts_crossing* out, int32_t capacity, int32_t* count, int64_t counts[2]) {
+  if (!surface || !count) return fail(MTS_ERR_ARG, "null argument");
+  mts_status st = check_params(grid, params);
+  if (st) return st;
+  std::unique_ptr<mts::Surface> surf(mts::make_surface(*surface));
+  if (!surf) return fail(MTS_ERR_ARG, "unknown surface kind");
+  mts::Grid g = mts::make_grid(*grid);
+  std::vector<int8_t> tg;
+  st = mts::build_tags(g, *surf, tg);
+  if (st) return fail(st, "a grid node lies on the interface");
+  std::vector<mts_crossing> cr;
+  mts::SetupReport rep;
+  st = mts::build_crossings(g, tg, *surf, params->beta_in, params->beta_out, params->mib, cr, &rep);
+  if (st) return fail(st, "interface setup failed (root finding, coherent corners, open surface or singular LU)");
+  if (tags) std::memcpy(tags, tg.data(), tg.size());
+  *count = (int32_t)cr.size();
+  if (out && capacity >= (int32_t)cr.size()) std::memcpy(out, cr.data(), cr.size() * sizeof(mts_crossing));
+  if (counts) {
+    counts[0] = rep.corner_pairs;
+    counts[1] = rep.singular_warnings;
+  }
+  return MTS_OK;
+}
+
+mts_status mts_destroy(mts_handle h) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  cudaStreamSynchronize(h->stream);
+  delete h;
+  return MTS_OK;
+}
+
+mts_status mts_initialize(mts_handle h) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  h->launches += mts::launch_initialize(h->dev, std::exp(-h->t), h->u0, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  return MTS_OK;
+}
+
+mts_status mts_set_solution(mts_handle h, const double* u) {
+  if (!h || !u) return fail(MTS_ERR_ARG, "null argument");
+  CUDA_TRY(cudaMemcpyAsync(h->u0, u, sizeof(double) * (size_t)h->g.nodes(), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return MTS_OK;
+}
+
+mts_status mts_get_solution(mts_handle h, double* u) {
+  if (!h || !u) return fail(MTS_ERR_ARG, "null argument");
+  CUDA_TRY(cudaMemcpyAsync(u, h->u0, sizeof(double) * (size_t)h->g.nodes(), cudaMemcpyDeviceToHost, h->stream));
+  return sync_status(h);
+}
+
+mts_status mts_solve_2nd(mts_handle h, double t_prev, double t_half, double t_next) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  return enqueue_step(h, t_prev, t_half, t_next);
+}
+
+mts_status mts_advance(mts_handle h, int32_t nsteps) {
+  if (!h || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
+  return advance(h, nsteps);
+}
+
+mts_status mts_advance_host(mts_handle h, const double* u_in, double* u_out, int32_t nsteps) {
+  if (!h || !u_in || !u_out || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
+  const size_t bytes = sizeof(double) * (size_t)h->g.nodes();
+  CUDA_TRY(cudaMemcpyAsync(h->u0, u_in, bytes, cudaMemcpyHostToDevice, h->stream));
+  mts_status st = advance(h, nsteps);
+  if (st) return st;
+  CUDA_TRY(cudaMemcpyAsync(u_out, h->u0, bytes, cudaMemcpyDeviceToHost, h->stream));
+  return sync_status(h);
+}
+
+mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  h->launches += mts::launch_norms(h->dev, std::exp(-h->t), h->u0, h->norm_part, h->norm_nb, h->norm_out, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(h->host_norm, h->norm_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  mts_status st = sync_status(h);
+  const double* r = h->host_norm;
+  if (lmax) *lmax = r[0];
+  if (l2) *l2 = r[2];
+  if (argmax3) {
+    long long key = (long long)r[1];
+    argmax3[2] = (int32_t)(key % h->g.nz);
+    key /= h->g.nz;
+    argmax3[1] = (int32_t)(key % h->g.ny);
+    argmax3[0] = (int32_t)(key / h->g.ny);
+  }
+  return st;
+}
+
+mts_status mts_get_time(mts_handle h, double* t) {
+  if (!h || !t) return fail(MTS_ERR_ARG, "null argument");
+  *t = h->t;
+  return MTS_OK;
+}
+
+mts_status mts_set_time(mts_handle h, double t) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  h->t = t;
+  return MTS_OK;
+}
+
+mts_status mts_synchronize(mts_handle h) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  return sync_status(h);
+}
+
+mts_status mts_get_counts(mts_handle h, int64_t counts[8]) {
+  if (!h || !counts) return fail(MTS_ERR_ARG, "null argument");
+  for (int d = 0; d < 3; d++) {
+    counts[d] = h->ncr[d];
+    counts[3 + d] = h->nblk[d];
+  }
+  counts[6] = h->rep.corner_pairs;
+  counts[7] = h->rep.singular_warnings;
+  return MTS_OK;
+}
+
+mts_status mts_export_tags(mts_handle h, int8_t* tags) {
+  if (!h || !tags) return fail(MTS_ERR_ARG, "null argument");
+  std::memcpy(tags, h->tags.data(), h->tags.size());
+  return MTS_OK;
+}
+
+mts_status mts_export_crossings(mts_handle h, mts_crossing* out, int32_t capacity, int32_t* count) {
+  if (!h || !count) return fail(MTS_ERR_ARG, "null argument");
+  *count = (int32_t)h->cross.size();
+  if (out) {
+    if (capacity < (int32_t)h->cross.size()) return fail(MTS_ERR_ARG, "capacity too small");
+    std::memcpy(out, h->cross.data(), h->cross.size() * sizeof(mts_crossing));
+  }
+  return MTS_OK;
+}
+
+mts_status mts_get_launch_count(mts_handle h, int64_t* launches) {
+  if (!h || !launches) return fail(MTS_ERR_ARG, "null argument");
+  *launches = h->launches;
+  return MTS_OK;
+}
+
+mts_status mts_set_profiling(mts_handle h, int32_t on) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  h->profiling = on != 0;
+  return MTS_OK;
+}
+
+mts_status mts_profile_read(mts_handle h, double ms[8], int64_t launches[8]) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (auto& a : h->ev_busy) {
+    for (int k = 0; k < h->slots(); k++) {
+      float v = 0;
+      CUDA_TRY(cudaEventElapsedTime(&v, a[2 * k], a[2 * k + 1]));
+      h->prof_ms[k] += v;
+      h->prof_n[k] += 1;
+    }
+    h->ev_free.push_back(a);
+  }
+  h->ev_busy.clear();
+  for (int k = 0; k < mts::kProfileSlots; k++) {
+    if (ms) ms[k] = h->prof_ms[k];
+    if (launches) launches[k] = h->prof_n[k];
+    h->prof_ms[k] = 0;
+    h->prof_n[k] = 0;
+  }
+  return MTS_OK;
+}
+
+mts_status mts_get_stream(mts_handle h, void** stream) {
+  if (!h || !stream) return fail(MTS_ERR_ARG, "null argument");
+  *stream = (void*)h->stream;
+  return MTS_OK;
+}
+
+}  // extern "C"

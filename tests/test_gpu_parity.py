@@ -1,0 +1,110 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's
+golden outputs and against the oracle.
+
+Tolerance: 1e-10 relative max-norm (max |u_gpu - u_ref| / max |u_ref|), the
+plain FP64 form's contract.  The kernels round every operation exactly as the
+reference build does, so the observed difference is expected to be 0; the
+tests also assert that, to catch any drift early."""
+import numpy as np
+import pytest
+
+import mts_b200 as M
+import oracle as O
+from conftest import load_golden, problem_from_dict, rel_maxdiff, spec_from_problem
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def run_gpu(spec, steps, tags=None, crossings=None, u0=None):
+    with M.Solver(spec, tags=tags, crossings=crossings) as s:
+        if u0 is None:
+            s.initialize()
+        else:
+            s.set_solution(u0)
+        s.advance(steps)
+        s.synchronize()
+        return s.solution(), s.norms(), s.time
+
+
+@pytest.mark.parametrize("path", ["own_setup", "reference_crossings"])
+def test_gpu_matches_golden(golden, path):
+    worst = 0.0
+    for name, entry in golden.items():
+        prob = problem_from_dict(entry["problem"])
+        u_ref, u0, tags, cr = load_golden(name)
+        spec = spec_from_problem(prob)
+        if path == "own_setup":
+            u, (lmax, l2, am), t = run_gpu(spec, prob.steps)
+        else:
+            u, (lmax, l2, am), t = run_gpu(spec, prob.steps, tags=tags, crossings=cr, u0=u0)
+        d = rel_maxdiff(u, u_ref)
+        worst = max(worst, d)
+        assert d <= TOL, f"{name}: relative max-norm difference {d:.3e}"
+        assert np.array_equal(u, u_ref), f"{name}: not bit-identical (rel {d:.3e})"
+        assert t == entry["info"]["t"]
+        assert lmax == entry["info"]["lmax"], name
+        assert abs(l2 - entry["info"]["l2"]) <= 1e-12 * max(1.0, entry["info"]["l2"]), name
+        assert list(am) == entry["info"]["argmax"], name
+    print(f"worst relative difference over {len(golden)} golden cases: {worst:.3e}")
+
+
+def test_gpu_initialize_matches_reference(golden):
+    for name, entry in golden.items():
+        prob = problem_from_dict(entry["problem"])
+        _, u0, _, _ = load_golden(name)
+        with M.Solver(spec_from_problem(prob)) as s:
+            s.initialize()
+            assert np.array_equal(s.solution(), u0), name
+
+
+RANDOM_CASES = []
+_rng = np.random.default_rng(0)
+for _i in range(8):
+    _n = tuple(int(v) for v in _rng.choice([17, 25, 33, 49, 65], size=3))
+    _ax = tuple(float(v) for v in _rng.uniform(0.3, 0.7, size=3))
+    _c = tuple(float(v) for v in _rng.uniform(-0.2, 0.2, size=3))
+    _bo = float(10 ** _rng.uniform(-3, 3))
+    _method = ["adi", "lod-ie", "lod-cn", "ts"][_i % 4]
+    RANDOM_CASES.append(dict(n=_n, surface_params=(*_ax, 1.0, *_c), beta_out=_bo, method=_method, mib=1 + (_i // 4)))
+
+
+@pytest.mark.parametrize("case", RANDOM_CASES, ids=[f"{c['method']}-l{c['mib']}-{c['n']}" for c in RANDOM_CASES])
+def test_gpu_matches_oracle_random_family(case):
+    """Problems drawn like the batched family (anisotropic grids, shifted
+    ellipsoids, beta_out log-uniform in [1e-3, 1e3]): GPU vs oracle."""
+    n = case["n"]
+    h = 2.0 / (min(n) - 1)
+    spec = M.Spec(n=n, surface_params=case["surface_params"], beta_in=1.0, beta_out=case["beta_out"],
+                  method=case["method"], mib=case["mib"], dt=h)
+    try:
+        tags, cr, _ = M.setup_host(spec)
+    except M.MtsError:
+        pytest.skip("geometry rejected by the reference setup rules")
+    prob = O.Problem(n=n, surface_params=case["surface_params"], beta_in=1.0, beta_out=case["beta_out"],
+                     method=case["method"], mib=case["mib"], dt=h, steps=5)
+    u0 = O.port_init(prob, tags)
+    u_or = O.port_run(prob, tags, cr, u0)
+    u, _, _ = run_gpu(spec, 5)
+    assert rel_maxdiff(u, u_or) <= TOL
+    assert np.array_equal(u, u_or)
+
+
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+@pytest.mark.parametrize("surface", ["ellipsoid", "torus"])
+def test_gpu_matches_oracle_65(method, surface):
+    """The drop-in configuration at 65^3 (beta 1:1000, dt = h) with MIB-L2,
+    a few steps, GPU vs oracle."""
+    sp = (0.7001, 0.4999, 0.4001, 1.0) if surface == "ellipsoid" else (0.5, 0.2)
+    spec = M.Spec(n=(65, 65, 65), surface=surface, surface_params=sp, beta_in=1.0, beta_out=1000.0, method=method,
+                  mib=2, dt=2.0 / 64)
+    tags, cr, _ = M.setup_host(spec)
+    prob = O.Problem(n=(65, 65, 65), surface=surface, surface_params=sp, beta_in=1.0, beta_out=1000.0,
+                     method=method, mib=2, dt=2.0 / 64, steps=3)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    u, (lmax, l2, am), t = run_gpu(spec, 3)
+    assert rel_maxdiff(u, u_or) <= TOL
+    assert np.array_equal(u, u_or)
+    lo, l2o, amo = O.port_norms(prob, tags, t, u_or)
+    assert lmax == lo and tuple(am) == amo
+    assert abs(l2 - l2o) <= 1e-12 * l2o
