@@ -37,13 +37,13 @@ METRIC = "cell-steps/s @256^3 plain FP64"
 # Algorithmic HBM bytes per grid node per launch of each kernel slot
 # (field reads/writes at 8 B plus the 1-byte node tag; scratch excluded).
 ALG_BYTES = {
-    "adi": {1: 17, 2: 17, 3: 25},
+    "adi": {1: 17, 2: 16, 3: 24, 4: 24},
     "lod-ie": {1: 17, 2: 17, 3: 17},
     "lod-cn": {1: 17, 2: 17, 3: 17},
     "ts": {1: 17, 2: 17, 3: 17, 4: 17, 5: 17},
 }
 SLOT_NAMES = {
-    "adi": ["jumps", "adi_x_sweep", "adi_y_sweep", "adi_z_sweep"],
+    "adi": ["jumps", "adi_rhs", "adi_x_sweep", "adi_y_sweep", "adi_z_sweep"],
     "lod-ie": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
     "lod-cn": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
     "ts": ["jumps", "ts_explicit_x", "ts_explicit_y", "ts_z_sweep", "ts_y_sweep", "ts_x_sweep"],
@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: auto)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default sweep shapes")
     return ap.parse_args()
 
 
@@ -252,6 +253,7 @@ def main():
     spec = M.Spec(**w)
     solver = M.Solver(spec)
     solver.initialize()
+    shapes = solver.autotune(2) if not a.no_autotune else (0, 0, 0)
     solver.advance(a.warmup)
     solver.synchronize()
 
@@ -344,6 +346,7 @@ def main():
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic exact solution, seeded geometry)",
         "config": config_of(w, world), "gpu_launches": int(launches), "kernels": kernels, "roofline": roofline,
+        "sweep_shapes": list(shapes),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * nodes,
                 "d2h_bytes_per_step": 8 * nodes, "steps": e2e_steps,
                 "api": "mts_advance_host (field uploaded and downloaded every step, pinned host memory)"},

@@ -171,6 +171,17 @@ mts_status mts_get_stream(mts_handle h, void** stream);
 mts_status mts_set_profiling(mts_handle h, int32_t on);
 mts_status mts_profile_read(mts_handle h, double ms[8], int64_t launches[8]);
 
+/* Launch shape of the persistent line-sweep kernels (rows staged per chunk,
+ * staging-ring depth, threads per CTA), chosen separately for the first,
+ * second and third implicit sweep of a step.  Every shape computes the same
+ * bits; they differ only in speed.  mts_autotune times each compiled shape on
+ * the handle's own problem for `steps` steps (the solution and time are
+ * restored afterwards) and keeps the fastest per sweep; shapes[3] receives
+ * the choice.  mts_sweep_shape_count gives the number of shapes. */
+int32_t mts_sweep_shape_count(void);
+mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape);
+mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
+
 /* Text of the last error on this thread. */
 const char* mts_last_error(void);
 

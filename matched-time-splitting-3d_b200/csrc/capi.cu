@@ -72,7 +72,7 @@ struct mts_problem {
   double prof_ms[mts::kProfileSlots] = {};
   int64_t prof_n[mts::kProfileSlots] = {};
 
-  int slots() const { return prm.method == MTS_TS ? 6 : 4; }
+  int slots() const { return prm.method == MTS_TS ? 6 : prm.method == MTS_ADI ? 5 : 4; }
 
   ~mts_problem() {
     if (stream) cudaStreamSynchronize(stream);
@@ -270,6 +270,7 @@ mts_status finish_create(mts_problem* h) {
       int side = h->tags[m] == 1;
       for (int z = 0; z < 3; z++) vdr[q][z] = D.vd[d][side][z];
       tag8[m] |= flag[d];
+      b.sides |= side << q;
     }
     precompute_block(b, D.cdt, vdr);
     blocks[d].push_back(b);
@@ -278,6 +279,120 @@ mts_status finish_create(mts_problem* h) {
   for (int d = 0; d < 3; d++) {
     for (size_t l = 0; l + 1 < bstart[d].size(); l++) bstart[d][l + 1] += bstart[d][l];
     h->nblk[d] = (int64_t)blocks[d].size();
+  }
+  // Thomas factorisation (the factor half of TDMA, douglas_adi.cc:1790-1798:
+  // gam_j = c_{j-1}/bet, bet = b_j - a_j*gam_j, same operations): prefix
+  // tables per direction and row-1 side, and per-node factors from the first
+  // MIB row on for the lines that cross the interface.
+  std::vector<double> ptab[3][2];
+  std::vector<double> fbet[3], fgam[3];
+  {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    std::vector<double> a, b, c;
+    auto factor = [&](int len, std::vector<double>& bet_out, std::vector<double>& gam_out) -> bool {
+      bet_out.resize(len);
+      gam_out.resize(len);
+      double bet = b[0];
+      if (bet == 0.0) return false;
+      bet_out[0] = bet;
+      gam_out[0] = 0.0;
+      for (int j = 1; j < len; j++) {
+        double gm = c[j - 1] / bet;
+        bet = b[j] - a[j] * gm;
+        if (bet == 0.0) return false;
+        gam_out[j] = gm;
+        bet_out[j] = bet;
+      }
+      return true;
+    };
+    std::vector<double> lb, lg;
+    for (int d = 0; d < 3; d++) {
+      const int len = n[d];
+      a.assign(len, 0.0);
+      b.assign(len, 1.0);
+      c.assign(len, 0.0);
+      for (int side = 0; side < 2; side++) {
+        for (int j = 1; j < len - 1; j++) {
+          a[j] = D.ia[d][side];
+          b[j] = D.ib[d][side];
+          c[j] = D.ic[d][side];
+        }
+        a[len - 1] = 0.0;
+        b[len - 1] = 1.0;
+        c[len - 1] = 0.0;
+        if (!factor(len, lb, lg)) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line factorisation");
+        ptab[d][side].resize(2 * (size_t)len);
+        for (int j = 0; j < len; j++) {
+          ptab[d][side][2 * j] = lb[j];
+          ptab[d][side][2 * j + 1] = lg[j];
+        }
+      }
+      if (blocks[d].empty()) continue;
+      fbet[d].assign((size_t)N, 0.0);
+      fgam[d].assign((size_t)N, 0.0);
+      const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+      const int n2 = n[a2];
+      for (size_t k = 0; k < blocks[d].size();) {
+        const int line = blocks[d][k].line;
+        const int i1 = line / n2, i2 = line % n2;
+        int idx3[3];
+        idx3[a1] = i1;
+        idx3[a2] = i2;
+        auto node = [&](int j) {
+          idx3[d] = j;
+          return g.index(idx3[0], idx3[1], idx3[2]);
+        };
+        a[0] = 0.0;
+        b[0] = 1.0;
+        c[0] = 0.0;
+        for (int j = 1; j < len - 1; j++) {
+          int side = h->tags[(size_t)node(j)] == 1;
+          a[j] = D.ia[d][side];
+          b[j] = D.ib[d][side];
+          c[j] = D.ic[d][side];
+        }
+        a[len - 1] = 0.0;
+        b[len - 1] = 1.0;
+        c[len - 1] = 0.0;
+        const int L1 = blocks[d][k].L;
+        for (; k < blocks[d].size() && blocks[d][k].line == line; k++) {
+          const mts::MibBlock& bk = blocks[d][k];
+          for (int q = 0; q < bk.kind; q++) {
+            a[bk.L + q] = bk.ia[q];
+            b[bk.L + q] = bk.ib[q];
+            c[bk.L + q] = bk.ic[q];
+          }
+        }
+        if (!factor(len, lb, lg)) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line factorisation");
+        for (int j = L1; j < len; j++) {
+          long long m = node(j);
+          fbet[d][(size_t)m] = lb[j];
+          fgam[d][(size_t)m] = lg[j];
+        }
+      }
+    }
+  }
+
+  // per-line side bits: node 0, node 1, node n-1 outside
+  std::vector<uint8_t> lside[3];
+  {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    for (int d = 0; d < 3; d++) {
+      const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+      const int n2 = n[a2];
+      lside[d].assign((size_t)line_count(g, d), 0);
+      for (int i1 = 0; i1 < n[a1]; i1++)
+        for (int i2 = 0; i2 < n[a2]; i2++) {
+          int idx3[3];
+          idx3[a1] = i1;
+          idx3[a2] = i2;
+          auto out_at = [&](int j) {
+            idx3[d] = j;
+            return h->tags[(size_t)g.index(idx3[0], idx3[1], idx3[2])] == 1 ? 1 : 0;
+          };
+          lside[d][(size_t)i1 * n2 + i2] = (uint8_t)(out_at(0) | (out_at(1) << 1) | (out_at(n[d] - 1) << 2));
+        }
+    }
   }
   for (size_t i = 0; i < h->cross.size(); i++) {
     const mts_crossing& c = h->cross[i];
@@ -309,16 +424,43 @@ mts_status finish_create(mts_problem* h) {
     }
   }
 
+  static bool configured = false;
+  if (!configured) {
+    mts::configure_kernels();
+    configured = true;
+  }
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  D.sweep_blocks = sms > 0 ? sms : 1;
+  for (int k = 0; k < 3; k++) D.shape[k] = 0;
+  const size_t tmax = (size_t)D.sweep_blocks * (size_t)mts::sweep_shape_max_threads();
+  const int nmax = std::max(g.nx, std::max(g.ny, g.nz));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   CUDA_TRY(h->put(&h->u0, (const double*)nullptr, (size_t)N));
   CUDA_TRY(h->put(&h->u1, (const double*)nullptr, (size_t)N));
-  CUDA_TRY(h->put(&D.gam, (const double*)nullptr, (size_t)N));
-  if (p.method == MTS_ADI) {
-    CUDA_TRY(h->put(&D.ydt, (const double*)nullptr, (size_t)N));
+  CUDA_TRY(h->put(&D.dp, (const double*)nullptr, (size_t)nmax * tmax));
+  for (int d = 0; d < 3; d++) {
+    for (int side = 0; side < 2; side++) {
+      double* pt = nullptr;
+      CUDA_TRY(h->put(&pt, ptab[d][side].data(), ptab[d][side].size()));
+      D.ptab[d][side] = pt;
+    }
+    double *fb = nullptr, *fg = nullptr;
+    if (!fbet[d].empty()) {
+      CUDA_TRY(h->put(&fb, fbet[d].data(), fbet[d].size()));
+      CUDA_TRY(h->put(&fg, fgam[d].data(), fgam[d].size()));
+    }
+    D.fbet[d] = fb;
+    D.fgam[d] = fg;
   }
   uint8_t* dtag = nullptr;
   CUDA_TRY(h->put(&dtag, tag8.data(), tag8.size()));
   D.tag = dtag;
+  for (int d = 0; d < 3; d++) {
+    uint8_t* ls = nullptr;
+    CUDA_TRY(h->put(&ls, lside[d].data(), lside[d].size()));
+    D.lside[d] = ls;
+  }
   for (int d = 0; d < 3; d++) {
     double *a = nullptr, *s = nullptr, *c = nullptr;
     CUDA_TRY(h->put(&a, axv[d].data(), axv[d].size()));
@@ -637,6 +779,59 @@ mts_status mts_profile_read(mts_handle h, double ms[8], int64_t launches[8]) {
     h->prof_n[k] = 0;
   }
   return MTS_OK;
+}
+
+int32_t mts_sweep_shape_count(void) { return mts::sweep_shape_count(); }
+
+mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape) {
+  if (!h || sweep < 0 || sweep > 2 || shape < 0 || shape >= mts::sweep_shape_count())
+    return fail(MTS_ERR_ARG, "bad sweep or shape index");
+  h->dev.shape[sweep] = shape;
+  return MTS_OK;
+}
+
+mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]) {
+  if (!h || steps < 1) return fail(MTS_ERR_ARG, "bad argument");
+  const size_t bytes = sizeof(double) * (size_t)h->g.nodes();
+  double* backup = nullptr;
+  CUDA_TRY(cudaMalloc((void**)&backup, bytes));
+  std::unique_ptr<double, decltype(&cudaFree)> guard(backup, &cudaFree);
+  CUDA_TRY(cudaMemcpyAsync(backup, h->u0, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  const double t0 = h->t;
+  const bool prof = h->profiling;
+  // profile slots of the three implicit sweeps
+  const int first = h->prm.method == MTS_ADI ? 2 : h->prm.method == MTS_TS ? 3 : 1;
+  double best[3] = {1e300, 1e300, 1e300};
+  int choice[3] = {0, 0, 0};
+  mts_status st = MTS_OK;
+  h->profiling = true;
+  for (int s = 0; s < mts::sweep_shape_count() && st == MTS_OK; s++) {
+    for (int k = 0; k < 3; k++) h->dev.shape[k] = s;
+    st = mts_profile_read(h, nullptr, nullptr);
+    if (st) break;
+    st = advance(h, steps);
+    if (st) break;
+    double ms[8];
+    int64_t cnt[8];
+    st = mts_profile_read(h, ms, cnt);
+    if (st) break;
+    for (int k = 0; k < 3; k++)
+      if (ms[first + k] < best[k]) {
+        best[k] = ms[first + k];
+        choice[k] = s;
+      }
+    CUDA_TRY(cudaMemcpyAsync(h->u0, backup, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    h->t = t0;
+  }
+  h->profiling = prof;
+  CUDA_TRY(cudaMemcpyAsync(h->u0, backup, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->t = t0;
+  for (int k = 0; k < 3; k++) {
+    h->dev.shape[k] = choice[k];
+    if (shapes) shapes[k] = choice[k];
+  }
+  return st;
 }
 
 mts_status mts_get_stream(mts_handle h, void** stream) {

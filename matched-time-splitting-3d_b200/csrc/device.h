@@ -3,12 +3,16 @@
 //
 // HBM layout of one problem (N = nx*ny*nz nodes, x fastest):
 //   u0, u1   float64[N]   solution ping-pong (state + stage results)
-//   gam      float64[N]   Thomas forward factors c_{j-1}/bet of the sweep in
-//                         flight (scratch, rewritten every sweep)
-//   ydt      float64[N]   Douglas-ADI: dt*D_yy u^n of the x sweep, read back
-//                         in that sweep's back substitution (scratch)
 //   tag      uint8[N]     bit0 outside, bit1/2/3 node is a MIB row of an
 //                         x/y/z crossing block
+//   gam, dp  float64[nmax x T]  Thomas forward factors c_{j-1}/bet and
+//                         partial solutions d'_j of the T = grid threads'
+//                         lines in flight, row-major [row][thread] so every
+//                         access is coalesced whatever the sweep direction;
+//                         reused line after line (~78 MB at 257 nodes and
+//                         148 x 128 threads: L2-resident)
+//   lside    uint8 per line and direction: bit0 node 0, bit1 node 1, bit2
+//                         node n-1 outside (the side changes only at crossings)
 //   per axis: coordinates, sin 2x, cos 2x (exact-solution tables)
 //   per direction: CSR offsets over grid lines -> MIB row blocks
 //   per crossing: time-invariant constants of its jump data, and the
@@ -32,7 +36,7 @@ struct MibBlock {
   int32_t L;
   int32_t kind;  // 2 or 3 rows
   int32_t c0, c1;
-  int32_t pad;
+  int32_t sides;  // bit q: row L+q is outside
   double w[4][9];
   double ia[3], ib[3], ic[3];
   double rate[6];
@@ -68,14 +72,32 @@ struct Dev {
   const double* s2[3];  // sin(2 x_i) per axis
   const double* c2[3];  // cos(2 x_i) per axis
   const uint8_t* tag;
+  const uint8_t* lside[3];
   const int32_t* bstart[3];
   const MibBlock* blk[3];
   const CrossConst* cc;
   double2* jv;  // per crossing ([u], u_dir) of the current step
-  double* gam;
-  double* ydt;
-  int* status;  // bit0: zero pivot in a line solve
+  // Thomas factorisation of every line, computed once (the matrices do not
+  // change between steps): bet_j = b_j - a_j*gam_j, gam_j = c_{j-1}/bet_{j-1}.
+  // Up to its first MIB row a line's factors depend only on the side of its
+  // row 1, so they come from the per-direction prefix tables
+  // ptab[d][side][2*j + {0: bet, 1: gam}]; from the first MIB row on they are
+  // stored per node in fbet[d] / fgam[d] (field layout, written only for
+  // lines that cross the interface).
+  const double* ptab[3][2];
+  const double* fbet[3];
+  const double* fgam[3];
+  double* dp;        // [nmax][sweep threads of the launch]: forward results d'_j
+  int sweep_blocks;  // one persistent CTA per SM
+  int shape[3];      // sweep shape of the first, second and third sweep of a step
+  int* status;       // reserved
 };
+
+// Persistent line-sweep shapes (rows per staged chunk, ring depth, threads
+// per CTA); all give bit-identical results, they differ only in speed.
+int sweep_shape_count();
+int sweep_shape_max_threads();
+void configure_kernels();
 
 // Per-step exact-solution time factors.
 struct StepTimes {

@@ -194,6 +194,16 @@ class Solver:
         check(self._L.mts_profile_read(self._h, ms.ctypes.data, n.ctypes.data), "mts_profile_read")
         return ms, n
 
+    def set_sweep_shape(self, sweep: int, shape: int) -> None:
+        check(self._L.mts_set_sweep_shape(self._h, int(sweep), int(shape)), "mts_set_sweep_shape")
+
+    def autotune(self, steps: int = 2):
+        """Times every compiled sweep shape on this problem and keeps the
+        fastest per sweep; the solution and time are left unchanged."""
+        out = np.zeros(3, dtype=np.int32)
+        check(self._L.mts_autotune(self._h, int(steps), out.ctypes.data), "mts_autotune")
+        return tuple(int(v) for v in out)
+
     def stream(self) -> int:
         v = ctypes.c_void_p()
         check(self._L.mts_get_stream(self._h, ctypes.byref(v)), "mts_get_stream")

@@ -50,6 +50,9 @@ EXPORTS = [
     "mts_get_stream",
     "mts_set_profiling",
     "mts_profile_read",
+    "mts_sweep_shape_count",
+    "mts_set_sweep_shape",
+    "mts_autotune",
     "mts_last_error",
     "mts_version",
 ]
@@ -163,6 +166,8 @@ def load(build_if_missing: bool = True):
             "mts_get_stream": [H, P(ctypes.c_void_p)],
             "mts_set_profiling": [H, ctypes.c_int32],
             "mts_profile_read": [H, vp, vp],
+            "mts_set_sweep_shape": [H, ctypes.c_int32, ctypes.c_int32],
+            "mts_autotune": [H, ctypes.c_int32, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -172,6 +177,8 @@ def load(build_if_missing: bool = True):
         L.mts_last_error.restype = ctypes.c_char_p
         L.mts_version.argtypes = []
         L.mts_version.restype = ctypes.c_int32
+        L.mts_sweep_shape_count.argtypes = []
+        L.mts_sweep_shape_count.restype = ctypes.c_int32
         _lib = L
         return L
 
