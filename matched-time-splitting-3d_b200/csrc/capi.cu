@@ -90,6 +90,17 @@ struct mts_problem {
     if (*dst) allocations.push_back((void*)*dst);
     return e;
   }
+  // n elements (uploaded from src when given) followed by `pad` zeroed
+  // elements of slack that the sweep kernels may read but never use
+  template <class T>
+  cudaError_t put_padded(T** dst, const T* src, size_t n, size_t pad) {
+    cudaError_t e = upload(dst, (const T*)nullptr, n + pad, stream);
+    if (*dst) allocations.push_back((void*)*dst);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(*dst + (src ? n : 0), 0, (src ? pad : n + pad) * sizeof(T), stream);
+    if (e != cudaSuccess || !src) return e;
+    return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream);
+  }
 };
 
 namespace {
@@ -432,23 +443,36 @@ mts_status finish_create(mts_problem* h) {
   int sms = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   D.sweep_blocks = sms > 0 ? sms : 1;
-  for (int k = 0; k < 3; k++) D.shape[k] = 0;
   const size_t tmax = (size_t)D.sweep_blocks * (size_t)mts::sweep_shape_max_threads();
   const int nmax = std::max(g.nx, std::max(g.ny, g.nz));
+  {
+    int def = -1;
+    for (int s = mts::sweep_shape_count() - 1; s >= 0; s--)
+      if (mts::sweep_shape_fits(s, nmax) && (def < 0 || s == 3)) def = s;
+    if (def < 0) return fail(MTS_ERR_ARG, "grid lines too long for the sweep kernels' shared memory");
+    for (int k = 0; k < 3; k++) D.shape[k] = def;
+  }
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  CUDA_TRY(h->put(&h->u0, (const double*)nullptr, (size_t)N));
-  CUDA_TRY(h->put(&h->u1, (const double*)nullptr, (size_t)N));
-  CUDA_TRY(h->put(&D.dp, (const double*)nullptr, (size_t)nmax * tmax));
+  // row slack of the fields the sweeps stage whole chunks of: kRowPad rows of
+  // the largest stride (an x-y plane)
+  const size_t fpad = (size_t)mts::kRowPad * (size_t)g.nx * (size_t)g.ny;
+  CUDA_TRY(h->put_padded(&h->u0, (const double*)nullptr, (size_t)N, fpad));
+  CUDA_TRY(h->put_padded(&h->u1, (const double*)nullptr, (size_t)N, fpad));
+  CUDA_TRY(h->put_padded(&D.dp, (const double*)nullptr, (size_t)nmax * tmax, (size_t)mts::kRowPad * tmax));
   for (int d = 0; d < 3; d++) {
     for (int side = 0; side < 2; side++) {
       double* pt = nullptr;
       CUDA_TRY(h->put(&pt, ptab[d][side].data(), ptab[d][side].size()));
       D.ptab[d][side] = pt;
     }
+    double* rbk = nullptr;
+    CUDA_TRY(h->put(&rbk, (const double*)nullptr, 3 * blocks[d].size()));
+    D.rblk[d] = rbk;
+    D.nblk[d] = (int)blocks[d].size();
     double *fb = nullptr, *fg = nullptr;
     if (!fbet[d].empty()) {
-      CUDA_TRY(h->put(&fb, fbet[d].data(), fbet[d].size()));
-      CUDA_TRY(h->put(&fg, fgam[d].data(), fgam[d].size()));
+      CUDA_TRY(h->put_padded(&fb, fbet[d].data(), fbet[d].size(), fpad));
+      CUDA_TRY(h->put_padded(&fg, fgam[d].data(), fgam[d].size(), fpad));
     }
     D.fbet[d] = fb;
     D.fgam[d] = fg;
@@ -786,6 +810,8 @@ int32_t mts_sweep_shape_count(void) { return mts::sweep_shape_count(); }
 mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape) {
   if (!h || sweep < 0 || sweep > 2 || shape < 0 || shape >= mts::sweep_shape_count())
     return fail(MTS_ERR_ARG, "bad sweep or shape index");
+  if (!mts::sweep_shape_fits(shape, std::max(h->g.nx, std::max(h->g.ny, h->g.nz))))
+    return fail(MTS_ERR_ARG, "shape needs more shared memory than this grid allows");
   h->dev.shape[sweep] = shape;
   return MTS_OK;
 }
@@ -805,7 +831,11 @@ mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]) {
   int choice[3] = {0, 0, 0};
   mts_status st = MTS_OK;
   h->profiling = true;
+  int choice0[3] = {h->dev.shape[0], h->dev.shape[1], h->dev.shape[2]};
+  for (int k = 0; k < 3; k++) choice[k] = choice0[k];
+  const int nmax = std::max(h->g.nx, std::max(h->g.ny, h->g.nz));
   for (int s = 0; s < mts::sweep_shape_count() && st == MTS_OK; s++) {
+    if (!mts::sweep_shape_fits(s, nmax)) continue;
     for (int k = 0; k < 3; k++) h->dev.shape[k] = s;
     st = mts_profile_read(h, nullptr, nullptr);
     if (st) break;

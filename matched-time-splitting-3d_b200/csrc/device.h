@@ -5,12 +5,16 @@
 //   u0, u1   float64[N]   solution ping-pong (state + stage results)
 //   tag      uint8[N]     bit0 outside, bit1/2/3 node is a MIB row of an
 //                         x/y/z crossing block
-//   gam, dp  float64[nmax x T]  Thomas forward factors c_{j-1}/bet and
-//                         partial solutions d'_j of the T = grid threads'
-//                         lines in flight, row-major [row][thread] so every
-//                         access is coalesced whatever the sweep direction;
-//                         reused line after line (~78 MB at 257 nodes and
-//                         148 x 128 threads: L2-resident)
+//   dp       float64[nmax x T]  partial solutions d'_j of the T = grid
+//                         threads' lines in flight, row-major [row][thread]
+//                         so every access is coalesced whatever the sweep
+//                         direction; reused line after line (L2-resident:
+//                         ~25 MB at 257 nodes and 148 x 256 threads)
+//   fbet, fgam float64[N] per direction that has crossings: Thomas factors
+//                         of crossing lines from their first MIB row on
+//   u0, u1, dp, fbet, fgam carry kRowPad rows of slack (an x-y plane per row
+//                         for the node fields) past their end: the sweeps
+//                         stage whole chunks of rows without bound checks
 //   lside    uint8 per line and direction: bit0 node 0, bit1 node 1, bit2
 //                         node n-1 outside (the side changes only at crossings)
 //   per axis: coordinates, sin 2x, cos 2x (exact-solution tables)
@@ -87,6 +91,11 @@ struct Dev {
   const double* ptab[3][2];
   const double* fbet[3];
   const double* fgam[3];
+  // Per block, for the sweep in flight: the right-hand sides of its rows after
+  // the jump terms and the Convert2Tri row operations, [3*block + q]
+  // (written by the block pre-pass, read by the sweep).
+  double* rblk[3];
+  int nblk[3];
   double* dp;        // [nmax][sweep threads of the launch]: forward results d'_j
   int sweep_blocks;  // one persistent CTA per SM
   int shape[3];      // sweep shape of the first, second and third sweep of a step
@@ -97,6 +106,7 @@ struct Dev {
 // per CTA); all give bit-identical results, they differ only in speed.
 int sweep_shape_count();
 int sweep_shape_max_threads();
+bool sweep_shape_fits(int shape, int nmax);  // shared memory of the shape within the limit
 void configure_kernels();
 
 // Per-step exact-solution time factors.
@@ -111,6 +121,7 @@ int launch_initialize(const Dev& P, double E, double* u, cudaStream_t stream);
 int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t stream,
                 cudaEvent_t* ev);
 constexpr int kProfileSlots = 8;
+constexpr int kRowPad = 16;  // rows of slack after each staged field (>= chunk rows)
 int launch_norms(const Dev& P, double E, const double* u, double* partial, int nblocks,
                  double* out3, cudaStream_t stream);
 int norms_blocks(const Dev& P);

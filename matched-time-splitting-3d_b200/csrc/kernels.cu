@@ -33,7 +33,8 @@
 namespace mts {
 namespace {
 
-constexpr int TPB = 128;  // pointwise kernels and small kernels
+constexpr int TPB = 128;                // pointwise kernels and small kernels
+constexpr int kMaxSweepSmem = 232448;  // 227 KB: the sm_100 per-CTA limit
 
 enum Kind { K_COPY = 0, K_STENCIL = 1, K_TS_Z = 2 };
 
@@ -371,16 +372,26 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit(const Dev P, const double* 
 // The persistent line sweep.  Shape: CH rows per staged chunk, NS chunks in
 // the ring (both powers of two), NT threads per CTA (one CTA per SM).
 //
-// Shared memory per thread column: three staged fields [NS*CH] (forward:
-// stencil field, added field, bet from the first MIB row on; backward: d'_j,
-// gam_{j+1}) and the right-hand sides of two chunks [2*CH].
+// Shared memory per thread column: three staged fields of NS*CH rows
+// (forward: stencil field, added field, bet from the first MIB row on;
+// backward: d'_j, gam_{j+1}).  Whole chunks are staged without per-row bound
+// checks: every field the sweep reads (the solution fields, the per-node
+// factors, the d' scratch) carries kRowPad rows of slack past its last row,
+// so the rows of a line's last chunk beyond n are readable (and never used).
+// The forward pass handles a chunk of regular rows (no MIB row, no line end)
+// with a fully unrolled loop at compile-time shared-memory offsets whose
+// stencil window slides in registers; chunks that hold a MIB block or a line
+// end take the row-by-row path.  The backward pass does the same for chunks
+// without the line end (and without the LOD epilogue).
 
 struct BlockHead {
   int L, kind, sides;
-  double a0, a1, a2;
+  double a0, a1, a2;  // sub-diagonal of the block's rows after Convert2Tri
+  double r0, r1, r2;  // their right-hand sides this sweep (block pre-pass)
 };
 
-__device__ __forceinline__ void load_head(const MibBlock* blk, int k, int end, BlockHead& h) {
+__device__ __forceinline__ void load_head(const MibBlock* blk, const double* rblk, int k, int end,
+                                          BlockHead& h) {
   if (k < end) {
     const MibBlock& b = blk[k];
     h.L = b.L;
@@ -389,6 +400,9 @@ __device__ __forceinline__ void load_head(const MibBlock* blk, int k, int end, B
     h.a0 = b.ia[0];
     h.a1 = b.ia[1];
     h.a2 = b.ia[2];
+    h.r0 = rblk[3 * k];
+    h.r1 = rblk[3 * k + 1];
+    h.r2 = rblk[3 * k + 2];
   } else {
     h.L = 0x7fffffff;
     h.kind = 0;
@@ -396,25 +410,119 @@ __device__ __forceinline__ void load_head(const MibBlock* blk, int k, int end, B
   }
 }
 
-template <int CH, int NS, int NT>
-constexpr size_t shape_smem() {
-  return sizeof(double) * (size_t)(3 * NS * CH * NT + 2 * CH * NT);
+// Block pre-pass of a sweep: one thread per MIB block of direction D computes
+// the right-hand sides of the block's rows exactly as the sweep would (the
+// explicit MIB stencil of douglas_adi.cc:112-210 / lod.cc:337-496, the jump
+// terms of D_xx_l lod.cc:960-1097, the Convert2Tri row operations) and stores
+// them for the sweep, which then spends no time on MIB data.
+template <int D, int KIND>
+__global__ void __launch_bounds__(TPB) k_block_rhs(const Dev P, const SweepIO io, int nblk) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= nblk) return;
+  const MibBlock& b = P.blk[D][k];
+  const int n2 = D == 2 ? P.ny : P.nz;
+  Line L;
+  decode_line<D>(P, (long long)(b.line % n2) * (D == 0 ? P.ny : P.nx) + b.line / n2, L);
+  const double* stin = KIND == K_COPY ? io.add : io.stin;
+  auto U = [&](int j) { return stin[L.base + (long long)j * L.s]; };
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < b.kind; q++) {
+    const int jj = b.L + q;
+    const int side = (b.sides >> q) & 1;
+    const double av = io.add[L.base + (long long)jj * L.s];
+    if (KIND == K_COPY) {
+      r[q] = av;
+    } else {
+      double sum = mib_sum(b, q, U, P.vd[D][side], io.jumps, P.jv);
+      double v = io.k * sum + av;
+      if (KIND == K_TS_Z) {
+        int ix, iy, iz;
+        node_of<D>(L, jj, ix, iy, iz);
+        v = v + P.hdt * source(P, io.e0, side, ix, iy, iz);
+        v = v + P.hdt * source(P, io.e1, side, ix, iy, iz);
+      }
+      r[q] = v;
+    }
+  }
+  implicit_rows(P, b, r, P.vd[D][b.sides & 1], P.vd[D][(b.sides >> 1) & 1], P.vd[D][(b.sides >> 2) & 1], io.jumps,
+                P.jv);
+  for (int q = 0; q < 3; q++) P.rblk[D][3 * k + q] = r[q];
 }
+
+// Exact-solution parts along a line: the fixed axes are read once per line,
+// the sweep axis from shared memory.  S = (sin2x cos2y) sin2z and
+// R2 = (x*x + y*y) + z*z keep the operand order of the exact-solution code,
+// so S*E and R2*E are the inner and outer solutions bit for bit.
+struct LineExact {
+  double x, y, z, s2x, c2y, s2z;
+};
+
+template <int D>
+__device__ __forceinline__ void line_exact(const Dev& P, const Line& L, LineExact& f) {
+  int ix, iy, iz;
+  node_of<D>(L, 0, ix, iy, iz);
+  f.x = P.ax[0][ix];
+  f.y = P.ax[1][iy];
+  f.z = P.ax[2][iz];
+  f.s2x = P.s2[0][ix];
+  f.c2y = P.c2[1][iy];
+  f.s2z = P.s2[2][iz];
+}
+
+// sX: [coordinate | sin 2x | cos 2x] of the sweep axis, nd rows each.
+template <int D>
+__device__ __forceinline__ void row_parts(const LineExact& f, const double* sX, int nd, int j, double& S,
+                                          double& R2) {
+  if (D == 0) {
+    const double x = sX[j];
+    S = (sX[nd + j] * f.c2y) * f.s2z;
+    R2 = (x * x + f.y * f.y) + f.z * f.z;
+  } else if (D == 1) {
+    const double y = sX[j];
+    S = (f.s2x * sX[2 * nd + j]) * f.s2z;
+    R2 = (f.x * f.x + y * y) + f.z * f.z;
+  } else {
+    const double z = sX[j];
+    S = (f.s2x * f.c2y) * sX[nd + j];
+    R2 = (f.x * f.x + f.y * f.y) + z * z;
+  }
+}
+__device__ __forceinline__ double outer_from(const Dev& P, double R2, double E) {
+  return P.eq == 0 ? 100.0 : R2 * E;
+}
+__device__ __forceinline__ double source_from(const Dev& P, double S, double R2, double E, int out) {
+  if (P.eq == 0) return 0.0;
+  if (out) return -(R2 * E) - P.c6bo * E;
+  return P.kin * (S * E);
+}
+
+// Shared memory of a shape: the staging ring, the two prefix factor tables
+// of the sweep direction (2 sides x 2 values x n rows) and its exact-solution
+// tables (3 x n).
+template <int CH, int NS, int NT>
+constexpr size_t shape_smem(int n) {
+  return sizeof(double) * ((size_t)3 * NS * CH * NT + (size_t)7 * n);
+}
+
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
 
 template <int D, int KIND, int CH, int NS, int NT>
 __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) {
   static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4, "shape");
-  constexpr int RING = NS * CH;
+  static_assert(CH <= kRowPad, "chunk rows past a line end must stay within the fields' slack");
+  constexpr int RING = NS * CH;    // rows in a field's ring
+  constexpr int SLOT = CH * NT;    // doubles per chunk slot
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
-  double* const sA = sm + tid;                  // [RING][NT]
-  double* const sB = sm + RING * NT + tid;      // [RING][NT]
-  double* const sC = sm + 2 * RING * NT + tid;  // [RING][NT]
-  double* const rb = sm + 3 * RING * NT + tid;  // [2*CH][NT]
+  double* const sA = sm + tid;             // [NS][CH][NT]
+  double* const sB = sA + NS * SLOT;       // [NS][CH][NT]
+  double* const sC = sB + NS * SLOT;       // [NS][CH][NT]
 #define SA(j) sA[((j) & (RING - 1)) * NT]
 #define SB(j) sB[((j) & (RING - 1)) * NT]
 #define SC(j) sC[((j) & (RING - 1)) * NT]
-#define RB(j) rb[((j) & (2 * CH - 1)) * NT]
   const long long T = (long long)gridDim.x * NT;
   const long long gt = (long long)blockIdx.x * NT + tid;
   double* const dp = P.dp + gt;
@@ -422,6 +530,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
   const MibBlock* __restrict__ blk = P.blk[D];
   const double* __restrict__ fbet = P.fbet[D];
   const double* __restrict__ fgam = P.fgam[D];
+  const double* __restrict__ rblk = P.rblk[D];
   const double E1 = io.e1;
   const double kx = io.k;
   // per-direction constants by side (0 inside, 1 outside), in registers
@@ -429,19 +538,35 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
   const double v1i = P.vd[D][0][1], v1o = P.vd[D][1][1];
   const double v2i = P.vd[D][0][2], v2o = P.vd[D][1][2];
   const double cai = P.ia[D][0], cao = P.ia[D][1];
+  // prefix factor tables [side][row][bet, gam] and exact-solution tables of
+  // the sweep axis [coordinate | sin 2x | cos 2x] into shared memory (they sit
+  // on the recurrence chain; the staging stream would evict them from L1)
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  double* const sP = sm + 3 * NS * SLOT;
+  double* const sX = sP + 4 * nd;
+  for (int i = tid; i < 4 * nd; i += NT) sP[i] = i < 2 * nd ? P.ptab[D][0][i] : P.ptab[D][1][i - 2 * nd];
+  for (int i = tid; i < nd; i += NT) {
+    sX[i] = P.ax[D][i];
+    sX[nd + i] = P.s2[D][i];
+    sX[2 * nd + i] = P.c2[D][i];
+  }
+  __syncthreads();
 
   for (long long t = gt; t < nl; t += T) {
     Line L;
     decode_line<D>(P, t, L);
     const int n = L.n;
+    const long long s = L.s;
+    LineExact fx;
+    line_exact<D>(P, L, fx);
     if (L.boundary) {
       if (io.bmode) {
         for (int j = 0; j < n; j++) {
-          int ix, iy, iz;
-          node_of<D>(L, j, ix, iy, iz);
-          long long m = L.base + (long long)j * L.s;
-          double v = outer_u(P, E1, ix, iy, iz);
-          if (io.bmode == 2) v = v + P.dt * source(P, E1, P.tag[m] & TAG_OUT, ix, iy, iz);
+          long long m = L.base + (long long)j * s;
+          double S, R2;
+          row_parts<D>(fx, sX, nd, j, S, R2);
+          double v = outer_from(P, R2, E1);
+          if (io.bmode == 2) v = v + P.dt * source_from(P, S, R2, E1, P.tag[m] & TAG_OUT);
           io.out[m] = v;
         }
       }
@@ -452,168 +577,166 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
     const int bfirst = P.bstart[D][L.lid];
     const int bend = P.bstart[D][L.lid + 1];
     const int L1 = bfirst < bend ? blk[bfirst].L : n;  // first MIB row
-    const double* __restrict__ pt = P.ptab[D][(ls >> 1) & 1];
-    // field A = the stencil field (or the copied field), field B = the added field
-    const double* fA = KIND == K_COPY ? io.add : io.stin;
-    const double* fB = io.add;
+    const double* pt = sP + ((ls >> 1) & 1) * 2 * nd;
     const bool two = KIND != K_COPY && io.add != io.stin;
-
+    // row j of a field: g[j*s]; rows up to nch*CH-1 are readable (the fields
+    // carry one chunk of slack past their end)
+    const double* gA = (KIND == K_COPY ? io.add : io.stin) + L.base;
+    const double* gB = io.add + L.base;
+    const double* gC = fbet + L.base;
     auto stage = [&](int c) {
       if (c < nch) {
-        long long off = L.base + (long long)c * CH * L.s;
+        const long long off = (long long)c * CH * s;
+        double* a = sA + (c & (NS - 1)) * SLOT;
 #pragma unroll
-        for (int r = 0; r < CH; r++) {
-          const int j = c * CH + r;
-          if (j < n) {
-            cp_async8(&SA(j), fA + off);
-            if (two) cp_async8(&SB(j), fB + off);
-            if (j >= L1) cp_async8(&SC(j), fbet + off);
-          }
-          off += L.s;
+        for (int r = 0; r < CH; r++) cp_async8(a + r * NT, gA + off + r * s);
+        if (two) {
+          double* b = sB + (c & (NS - 1)) * SLOT;
+#pragma unroll
+          for (int r = 0; r < CH; r++) cp_async8(b + r * NT, gB + off + r * s);
+        }
+        if ((c + 1) * CH > L1) {
+          double* cc = sC + (c & (NS - 1)) * SLOT;
+#pragma unroll
+          for (int r = 0; r < CH; r++) cp_async8(cc + r * NT, gC + off + r * s);
         }
       }
       cp_async_commit();
     };
-
-    // right-hand side of chunk c into RB; r-pass block cursor and side
-    int rbk = bfirst;
-    int rbL = L1 < n ? L1 : 0x7fffffff;
-    int rside = (ls >> 1) & 1;
-    auto compute_r = [&](int c) {
-#pragma unroll 2
-      for (int rr = 0; rr < CH; rr++) {
-        const int j = c * CH + rr;
-        if (j >= n) break;
-        double r;
-        if (j == 0 || j == n - 1) {
-          int ix, iy, iz;
-          node_of<D>(L, j, ix, iy, iz);
-          r = outer_u(P, E1, ix, iy, iz);
-        } else if (j < rbL) {
-          // regular row
-          if (KIND == K_COPY) {
-            r = SA(j);
-          } else {
-            double sum = 0.0;
-            sum += SA(j - 1) * (rside ? v0o : v0i);
-            sum += SA(j) * (rside ? v1o : v1i);
-            sum += SA(j + 1) * (rside ? v2o : v2i);
-            r = kx * sum + (two ? SB(j) : SA(j));
-            if (KIND == K_TS_Z) {
-              int ix, iy, iz;
-              node_of<D>(L, j, ix, iy, iz);
-              r = r + P.hdt * source(P, io.e0, rside, ix, iy, iz);
-              r = r + P.hdt * source(P, E1, rside, ix, iy, iz);
-            }
-          }
-        } else {
-          // a MIB row of the line's next block
-          const MibBlock& b = blk[rbk];
-          const int q = j - rbL;
-          const int side = (b.sides >> q) & 1;
-          if (KIND == K_COPY) {
-            r = SA(j);
-          } else {
-            const double* vd = P.vd[D][side];
-            double sum = mib_sum(b, q, [&](int jj) { return SA(jj); }, vd, io.jumps, P.jv);
-            r = kx * sum + (two ? SB(j) : SA(j));
-            if (KIND == K_TS_Z) {
-              int ix, iy, iz;
-              node_of<D>(L, j, ix, iy, iz);
-              r = r + P.hdt * source(P, io.e0, side, ix, iy, iz);
-              r = r + P.hdt * source(P, E1, side, ix, iy, iz);
-            }
-          }
-          if (q == b.kind - 1) {
-            rside = side;
-            rbk++;
-            rbL = rbk < bend ? blk[rbk].L : 0x7fffffff;
-          }
-        }
-        RB(j) = r;
+    auto outer_at = [&](int j) -> double {
+      double S, R2;
+      row_parts<D>(fx, sX, nd, j, S, R2);
+      return outer_from(P, R2, E1);
+    };
+    // right-hand side of a regular row from its stencil values
+    auto rhs = [&](int j, double xm, double x0, double xp, double addv, double w0, double w1, double w2,
+                   int side) -> double {
+      if (KIND == K_COPY) return x0;
+      double sum = 0.0;
+      sum += xm * w0;
+      sum += x0 * w1;
+      sum += xp * w2;
+      double r = kx * sum + addv;
+      if (KIND == K_TS_Z) {
+        double S, R2;
+        row_parts<D>(fx, sX, nd, j, S, R2);
+        r = r + P.hdt * source_from(P, S, R2, io.e0, side);
+        r = r + P.hdt * source_from(P, S, R2, E1, side);
       }
+      return r;
     };
 
-    // MIB row mixing for the blocks that start in chunk c
-    int xb = bfirst;
-    auto mix = [&](int c) {
-      while (xb < bend && blk[xb].L < (c + 1) * CH) {
-        const MibBlock& b = blk[xb];
-        double r[3];
-        for (int q = 0; q < b.kind; q++) r[q] = RB(b.L + q);
-        implicit_rows(P, b, r, P.vd[D][b.sides & 1], P.vd[D][(b.sides >> 1) & 1], P.vd[D][(b.sides >> 2) & 1],
-                      io.jumps, P.jv);
-        for (int q = 0; q < b.kind; q++) RB(b.L + q) = r[q];
-        xb++;
-      }
-    };
-
-    // forward substitution with the precomputed factors (TDMA,
+    // ---- forward substitution with the precomputed factors (TDMA,
     // douglas_adi.cc:1794-1800): d'_j = (r_j - a_j d'_{j-1}) / bet_j
+    for (int c = 0; c < NS - 2; c++) stage(c);
     int mb = bfirst;
-    BlockHead hb;
-    load_head(blk, mb, bend, hb);
+    BlockHead hb, hb2;  // the next block and the one after (prefetched)
+    load_head(blk, rblk, mb, bend, hb);
+    load_head(blk, rblk, mb + 1, bend, hb2);
     int mside = (ls >> 1) & 1;
     double dprev = 0.0;
-    double* dq = dp;
-    auto forward = [&](int c) {
-#pragma unroll 2
-      for (int rr = 0; rr < CH; rr++) {
-        const int j = c * CH + rr;
-        if (j >= n) break;
-        const double r = RB(j);
-        double d;
-        if (j == 0) {
-          d = r / pt[0];
-        } else {
-          double a;
-          if (j >= hb.L) {
-            const int q = j - hb.L;
-            a = q == 0 ? hb.a0 : q == 1 ? hb.a1 : hb.a2;
-            if (q == hb.kind - 1) {
-              mside = (hb.sides >> q) & 1;
-              mb++;
-              load_head(blk, mb, bend, hb);
-            }
-          } else if (j == n - 1) {
-            a = 0.0;
-          } else {
-            a = mside ? cao : cai;
-          }
-          const double bet = j >= L1 ? SC(j) : pt[2 * j];
-          d = (r - a * dprev) / bet;
-        }
-        *dq = d;
-        dq += T;
-        dprev = d;
-      }
-    };
-
-    for (int c = 0; c < NS - 1; c++) stage(c);
-    cp_async_wait<NS - 3>();
-    compute_r(0);
+    int j = 1;
     for (int c = 0; c < nch; c++) {
-      stage(c + NS - 1);
-      cp_async_wait<NS - 3>();
-      if (c + 1 < nch) compute_r(c + 1);
-      mix(c);
-      forward(c);
+      stage(c + NS - 2);
+      cp_async_wait<NS - 3>();  // chunks c-1, c, c+1 resident
+      if (c == 0) {
+        dprev = outer_at(0) / pt[0];
+        dp[0] = dprev;
+      }
+      const int c0 = c * CH;
+      const int cend = min(c0 + CH, n - 1);
+      if (j >= cend) continue;
+      if (j == c0 && cend == c0 + CH && hb.L >= cend && (cend <= L1 || c0 >= L1)) {
+        // a chunk of regular rows, same side, factors from one source
+        const double w0 = mside ? v0o : v0i, w1 = mside ? v1o : v1i, w2 = mside ? v2o : v2i;
+        const double ac = mside ? cao : cai;
+        const double* a = sA + (c & (NS - 1)) * SLOT;
+        const double* ap = sA + ((c - 1) & (NS - 1)) * SLOT;
+        const double* an = sA + ((c + 1) & (NS - 1)) * SLOT;
+        const double* b = sB + (c & (NS - 1)) * SLOT;
+        double* q = dp + (long long)c0 * T;
+        auto run = [&](auto tag) {
+          // tag: bet from the staged per-node factors, else from the prefix table
+          constexpr bool kField = decltype(tag)::value;
+          const double* bt = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0;
+          double xm = ap[(CH - 1) * NT];
+          double x0 = a[0];
+#pragma unroll
+          for (int rr = 0; rr < CH; rr++) {
+            const double xp = rr == CH - 1 ? an[0] : a[(rr + 1) * NT];
+            const double r = rhs(c0 + rr, xm, x0, xp, two ? b[rr * NT] : x0, w0, w1, w2, mside);
+            const double bet = kField ? bt[rr * NT] : bt[2 * rr];
+            const double d = (r - ac * dprev) / bet;
+            q[rr * T] = d;
+            dprev = d;
+            xm = x0;
+            x0 = xp;
+          }
+        };
+        if (c0 >= L1)
+          run(BoolC<true>{});
+        else
+          run(BoolC<false>{});
+        j = cend;
+      } else {
+        while (j < cend) {
+          const double bet = j >= L1 ? SC(j) : pt[2 * j];
+          if (j == hb.L) {
+            // a MIB block: its rows' right-hand sides come mixed from the
+            // block pre-pass (k_block_rhs); substitute them
+            double d = (hb.r0 - hb.a0 * dprev) / bet;
+            dp[(long long)j * T] = d;
+            dprev = d;
+            d = (hb.r1 - hb.a1 * dprev) / SC(j + 1);
+            dp[(long long)(j + 1) * T] = d;
+            dprev = d;
+            if (hb.kind == 3) {
+              d = (hb.r2 - hb.a2 * dprev) / SC(j + 2);
+              dp[(long long)(j + 2) * T] = d;
+              dprev = d;
+            }
+            mside = (hb.sides >> (hb.kind - 1)) & 1;
+            j += hb.kind;
+            mb++;
+            hb = hb2;
+            load_head(blk, rblk, mb + 1, bend, hb2);
+          } else {
+            const double r = rhs(j, SA(j - 1), SA(j), SA(j + 1), two ? SB(j) : SA(j), mside ? v0o : v0i,
+                                 mside ? v1o : v1i, mside ? v2o : v2i, mside);
+            const double d = (r - (mside ? cao : cai) * dprev) / bet;
+            dp[(long long)j * T] = d;
+            dprev = d;
+            j++;
+          }
+        }
+      }
     }
+    {
+      // last row: the Dirichlet identity row (a = 0)
+      const double r = outer_at(n - 1);
+      const double a = 0.0;
+      const double bet = n - 1 >= L1 ? SC(n - 1) : pt[2 * (n - 1)];
+      dp[(long long)(n - 1) * T] = (r - a * dprev) / bet;
+    }
+    cp_async_wait<0>();
 
-    // back substitution u_j = d'_j - gam_{j+1} u_{j+1} (douglas_adi.cc:
+    // ---- back substitution u_j = d'_j - gam_{j+1} u_{j+1} (douglas_adi.cc:
     // 1805-1806), staged back through the ring: field A = d'_j, field B =
     // gam_{j+1} where it comes from the per-node factors.  The fence orders
     // this thread's d' stores before the asynchronous copies that read them.
     __threadfence_block();
+    const double* gG = fgam + L.base;
     auto bstage = [&](int c) {
       if (c >= 0) {
+        double* a = sA + (c & (NS - 1)) * SLOT;
+        const double* g = dp + (long long)c * CH * T;
 #pragma unroll
-        for (int r = 0; r < CH; r++) {
-          const int j = c * CH + r;
-          if (j < n) {
-            cp_async8(&SA(j), dp + (long long)j * T);
-            if (j + 1 < n && j + 1 >= L1) cp_async8(&SB(j), fgam + L.base + (long long)(j + 1) * L.s);
-          }
+        for (int r = 0; r < CH; r++) cp_async8(a + r * NT, g + r * T);
+        if ((c + 1) * CH >= L1) {
+          double* b = sB + (c & (NS - 1)) * SLOT;
+          const long long off = ((long long)c * CH + 1) * s;
+#pragma unroll
+          for (int r = 0; r < CH; r++) cp_async8(b + r * NT, gG + off + r * s);
         }
       }
       cp_async_commit();
@@ -630,45 +753,66 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
     for (int c = nch - 1; c >= 0; c--) {
       bstage(c - NS + 1);
       cp_async_wait<NS - 1>();
-#pragma unroll 2
-      for (int rr = CH - 1; rr >= 0; rr--) {
-        const int j = c * CH + rr;
-        if (j >= n) continue;
-        double u = SA(j);
-        if (j != n - 1) {
-          const double gm = j + 1 >= L1 ? SB(j) : pt[2 * (j + 1) + 1];
-          u -= gm * unext;
-        }
-        unext = u;
-        double v = u;
-        if (io.last) {
-          int side;
-          if (j == 0) {
-            side = ls & 1;
-          } else if (j == n - 1) {
-            side = (ls >> 2) & 1;
-          } else if (j >= dbL && j < dbL + dbK) {
-            side = (dbS >> (j - dbL)) & 1;
-            if (j == dbL) {
-              dside = dbS & 1;
-              db--;
-              if (db >= bfirst) {
-                dbL = blk[db].L;
-                dbK = blk[db].kind;
-                dbS = blk[db].sides;
-              } else {
-                dbL = -1;
-                dbK = 0;
-              }
-            }
-          } else {
-            side = dside;
+      const int c0 = c * CH;
+      if (!io.last && c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
+        // every row has a successor; gam_{j+1} from one source
+        const double* a = sA + (c & (NS - 1)) * SLOT;
+        double* o = io.out + L.base + (long long)c0 * s;
+        auto run = [&](auto tag) {
+          // tag: gam_{j+1} from the staged per-node factors, else from the
+          // prefix table (pt + 2*c0 + 3 is gam of row c0 + 1)
+          constexpr bool kField = decltype(tag)::value;
+          const double* gb = kField ? sB + (c & (NS - 1)) * SLOT : pt + 2 * c0 + 3;
+#pragma unroll
+          for (int rr = CH - 1; rr >= 0; rr--) {
+            const double gm = kField ? gb[rr * NT] : gb[2 * rr];
+            double u = a[rr * NT];
+            u -= gm * unext;
+            unext = u;
+            o[rr * s] = u;
           }
-          int ix, iy, iz;
-          node_of<D>(L, j, ix, iy, iz);
-          v = u + P.dt * source(P, E1, side, ix, iy, iz);
+        };
+        if (c0 + 1 >= L1)
+          run(BoolC<true>{});
+        else
+          run(BoolC<false>{});
+      } else {
+        for (int rr = CH - 1; rr >= 0; rr--) {
+          const int jj = c0 + rr;
+          if (jj >= n) continue;
+          double u = SA(jj);
+          if (jj != n - 1) u -= (jj + 1 >= L1 ? SB(jj) : pt[2 * (jj + 1) + 1]) * unext;
+          unext = u;
+          double v = u;
+          if (io.last) {
+            int side;
+            if (jj == 0) {
+              side = ls & 1;
+            } else if (jj == n - 1) {
+              side = (ls >> 2) & 1;
+            } else if (jj >= dbL && jj < dbL + dbK) {
+              side = (dbS >> (jj - dbL)) & 1;
+              if (jj == dbL) {
+                dside = dbS & 1;
+                db--;
+                if (db >= bfirst) {
+                  dbL = blk[db].L;
+                  dbK = blk[db].kind;
+                  dbS = blk[db].sides;
+                } else {
+                  dbL = -1;
+                  dbK = 0;
+                }
+              }
+            } else {
+              side = dside;
+            }
+            double S, R2;
+            row_parts<D>(fx, sX, nd, jj, S, R2);
+            v = u + P.dt * source_from(P, S, R2, E1, side);
+          }
+          io.out[L.base + (long long)jj * s] = v;
         }
-        io.out[L.base + (long long)j * L.s] = v;
       }
     }
     cp_async_wait<0>();
@@ -676,7 +820,6 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
 #undef SA
 #undef SB
 #undef SC
-#undef RB
 }
 
 // Refresh_Jump (intersection.cc:2294-2490): [u] and u_dir per crossing.
@@ -780,15 +923,17 @@ unsigned pointwise_blocks(const Dev& P) {
 
 // Sweep shapes (rows per chunk, ring chunks, threads per CTA), selected per
 // sweep of a step by Dev::shape (mts_set_sweep_shape / mts_autotune).
-#define MTS_SHAPES(X) X(0, 16, 4, 128) X(1, 8, 8, 128) X(2, 8, 4, 256) X(3, 4, 8, 256) X(4, 8, 4, 192)
+#define MTS_SHAPES(X) X(0, 8, 8, 128) X(1, 4, 16, 128) X(2, 4, 8, 256) X(3, 8, 4, 256) X(4, 4, 8, 192) X(5, 4, 8, 288)
 
 template <int D, int KIND, int CH, int NS, int NT>
 void sweep_shape(const Dev& P, const SweepIO& io, cudaStream_t st) {
-  k_sweep<D, KIND, CH, NS, NT><<<P.sweep_blocks, NT, shape_smem<CH, NS, NT>(), st>>>(P, io);
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  k_sweep<D, KIND, CH, NS, NT><<<P.sweep_blocks, NT, shape_smem<CH, NS, NT>(nd), st>>>(P, io);
 }
 
 template <int D, int KIND>
 void sweep(const Dev& P, const SweepIO& io, int shape, cudaStream_t st) {
+  if (P.nblk[D] > 0) k_block_rhs<D, KIND><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, io, P.nblk[D]);
   switch (shape) {
 #define MTS_CASE(id, ch, ns, nt) \
   case id:                       \
@@ -805,15 +950,27 @@ template <int D, int KIND>
 void set_smem_attr() {
 #define MTS_ATTR(id, ch, ns, nt)                                                             \
   cudaFuncSetAttribute(k_sweep<D, KIND, ch, ns, nt>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                       (int)shape_smem<ch, ns, nt>());
+                       kMaxSweepSmem);
   MTS_SHAPES(MTS_ATTR)
 #undef MTS_ATTR
 }
 
 }  // namespace
 
-int sweep_shape_count() { return 5; }
-int sweep_shape_max_threads() { return 256; }
+int sweep_shape_count() { return 6; }
+
+bool sweep_shape_fits(int shape, int nmax) {
+  switch (shape) {
+#define MTS_FITS(id, ch, ns, nt) \
+  case id:                       \
+    return shape_smem<ch, ns, nt>(nmax) <= (size_t)kMaxSweepSmem;
+    MTS_SHAPES(MTS_FITS)
+#undef MTS_FITS
+    default:
+      return false;
+  }
+}
+int sweep_shape_max_threads() { return 288; }
 
 void configure_kernels() {
   set_smem_attr<0, K_COPY>();
@@ -944,6 +1101,9 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
     mark(1);
     launches += 5;
   }
+  // every method sweeps each direction once; each sweep with MIB blocks is
+  // preceded by its block pre-pass
+  for (int d = 0; d < 3; d++) launches += P.nblk[d] > 0;
   return launches;
 }
 
