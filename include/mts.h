@@ -137,6 +137,28 @@ mts_status mts_advance_host(mts_handle h, const double* u_in, double* u_out, int
  * exact solution at the current time.  Synchronous. */
 mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3);
 
+/* The same norms with no allocation of any kind.  This entry point has no
+ * counterpart in the reference.  It is for host programs that keep fields in
+ * a device pool of their own (a framework's caching allocator holding most of
+ * HBM, a process under a hard memory cap) and check their error mid-run,
+ * where a cudaMalloc may fail and a cudaFree would synchronize the device.
+ *
+ * u_dev: a device field of nx*ny*nz doubles laid out like the solution,
+ * evaluated against the exact solution at time t; NULL evaluates the handle's
+ * own solution at the handle's time (t ignored).  The outputs equal
+ * mts_norms' bit for bit.  Synchronous on the handle's stream.
+ *
+ * The reduction's scratch is one static device array of 48.5 KiB per device,
+ * holding the partials of at most 2048 reduction blocks: grids of more than
+ * 4194304 nodes (2048 x 2048) are rejected with MTS_ERR_ARG.  Its ticket
+ * counter must be zero when the kernel starts; each call clears it first.
+ * All calls on a device share the array, so calls that overlap in time on one
+ * device (other handles, streams or host threads) race: serialise them.  The
+ * first call on a device looks the array's address up (and may load the
+ * module); make that call before any stream capture begins on the device. */
+mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double* lmax, double* l2,
+                             int32_t* argmax3);
+
 mts_status mts_get_time(mts_handle h, double* t);
 mts_status mts_set_time(mts_handle h, double t);
 

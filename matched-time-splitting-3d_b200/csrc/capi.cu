@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -715,6 +716,66 @@ mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3) {
   CUDA_TRY(cudaMemcpyAsync(h->host_norm, h->norm_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   mts_status st = sync_status(h);
   const double* r = h->host_norm;
+  if (lmax) *lmax = r[0];
+  if (l2) *l2 = r[2];
+  if (argmax3) {
+    long long key = (long long)r[1];
+    argmax3[2] = (int32_t)(key % h->g.nz);
+    key /= h->g.nz;
+    argmax3[1] = (int32_t)(key % h->g.ny);
+    argmax3[0] = (int32_t)(key / h->g.ny);
+  }
+  return st;
+}
+
+// Norms with no allocation.  Who needs it: a host program that keeps its own
+// fields in a device pool it manages (a framework's caching allocator that
+// has reserved most of HBM, a service under a hard memory cap) and checks
+// their error mid-run, where a cudaMalloc may fail for want of free memory
+// and a cudaFree would synchronize the whole device.  It reuses nothing the
+// handle allocated for mts_norms: the reduction scratch is the module's
+// static array, whose device address is looked up once per device, with that
+// device current, and then cached.  The first call on a device therefore
+// does one runtime lookup (which may load the module); make it before any
+// stream capture starts on that device.
+mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double* lmax, double* l2,
+                             int32_t* argmax3) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  const int nb = mts::norms_blocks(h->dev);
+  if (nb > mts::kNoAllocMaxBlocks)
+    return fail(MTS_ERR_ARG, "mts_norms_noalloc: a grid of " + std::to_string(h->g.nodes()) + " nodes needs " +
+                                 std::to_string(nb) + " reduction blocks; the static scratch holds " +
+                                 std::to_string(mts::kNoAllocMaxBlocks) + " (grids of at most " +
+                                 std::to_string((long long)mts::kNoAllocMaxBlocks * 2048) + " nodes)");
+  constexpr int kMaxDevices = 64;
+  if (h->device < 0 || h->device >= kMaxDevices) return fail(MTS_ERR_ARG, "device ordinal out of range");
+  static std::mutex lock;
+  static double* addr[kMaxDevices] = {};
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(lock);
+    if (!addr[h->device]) {
+      int cur = -1;
+      CUDA_TRY(cudaGetDevice(&cur));
+      if (cur != h->device) CUDA_TRY(cudaSetDevice(h->device));
+      double* p = nullptr;
+      cudaError_t e = mts::noalloc_scratch_address(&p);
+      if (cur != h->device) cudaSetDevice(cur);
+      if (e != cudaSuccess)
+        return fail(MTS_ERR_CUDA, std::string("cudaGetSymbolAddress(static norms scratch): ") + cudaGetErrorString(e));
+      addr[h->device] = p;
+    }
+    scratch = addr[h->device];
+  }
+  const double* u = u_dev ? u_dev : h->u0;
+  const double tt = u_dev ? t : h->t;
+  // the ticket counter must start at zero
+  CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned), h->stream));
+  h->launches += mts::launch_norms_noalloc(h->dev, std::exp(-tt), u, scratch, nb, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  double r[3];
+  CUDA_TRY(cudaMemcpyAsync(r, scratch + 32, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+  mts_status st = sync_status(h);
   if (lmax) *lmax = r[0];
   if (l2) *l2 = r[2];
   if (argmax3) {

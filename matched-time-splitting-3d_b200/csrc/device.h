@@ -126,4 +126,13 @@ int launch_norms(const Dev& P, double E, const double* u, double* partial, int n
                  double* out3, cudaStream_t stream);
 int norms_blocks(const Dev& P);
 
+// Error norms through a statically sized module array instead of handle
+// buffers (mts_norms_noalloc).  The array holds the ticket counter, the
+// result triple and the partials of at most kNoAllocMaxBlocks blocks, i.e.
+// grids of at most kNoAllocMaxBlocks * 2048 nodes (norms_blocks).
+constexpr int kNoAllocMaxBlocks = 2048;
+constexpr int kNoAllocScratchDoubles = 64 + 3 * kNoAllocMaxBlocks;  // 48.5 KiB
+cudaError_t noalloc_scratch_address(double** p);  // call with the device current
+int launch_norms_noalloc(const Dev& P, double E, const double* u, double* scratch, int nb, cudaStream_t stream);
+
 }  // namespace mts

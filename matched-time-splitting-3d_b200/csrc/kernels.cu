@@ -1107,4 +1107,101 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
   return launches;
 }
 
+// ---------------------------------------------------------------------------
+// Error norms with no allocation (mts_norms_noalloc).  A caller that cannot
+// allocate device memory still needs somewhere for the per-block partials of
+// the reduction, so they live in one statically sized module array instead
+// of a buffer owned by a handle.  Layout, in doubles:
+//   [0]        ticket counter (read as unsigned): MUST be zero when the
+//              kernel starts; the host clears it before each launch and the
+//              last block leaves it at zero
+//   [32..34]   the result triple (max |e|, argmax key, L2)
+//   [64 ..)    3 doubles of partials per block, kNoAllocMaxBlocks blocks
+// Every call on a device uses the same array, so calls that overlap in time
+// on one device (two handles, two streams, two host threads) race.
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+cudaError_t noalloc_scratch_address(double** p) { return cudaGetSymbolAddress((void**)p, g_noalloc_scratch); }
+
+namespace {
+
+// One launch: each block reduces its share exactly as k_norms_partial does;
+// the block that takes the last ticket then combines the partials exactly as
+// k_norms_final does, so the triple is bit-identical to launch_norms' with
+// the same block count.
+__global__ void __launch_bounds__(NB_TPB) k_norms_noalloc(const Dev P, double E, const double* u, double* scratch) {
+  __shared__ double smax[NB_TPB], ssum[NB_TPB];
+  __shared__ long long skey[NB_TPB];
+  __shared__ int last;
+  unsigned* const ticket = reinterpret_cast<unsigned*>(scratch);
+  double* const res = scratch + 32;
+  double* const part = scratch + 64;
+  double vmax = 0.0, vsum = 0.0;
+  long long vkey = 0x7fffffffffffffffLL;
+  for (long long m = (long long)blockIdx.x * NB_TPB + threadIdx.x; m < P.nn; m += (long long)gridDim.x * NB_TPB) {
+    int ix, iy, iz;
+    node_xyz(P, m, ix, iy, iz);
+    double ex = (P.tag[m] & TAG_OUT) ? outer_u(P, E, ix, iy, iz) : inner_u(P, E, ix, iy, iz);
+    double e = fabs(u[m] - ex);
+    long long key = ((long long)ix * P.ny + iy) * P.nz + iz;
+    better(vmax, vkey, e, key);
+    vsum += e * e;
+  }
+  smax[threadIdx.x] = vmax;
+  skey[threadIdx.x] = vkey;
+  ssum[threadIdx.x] = vsum;
+  __syncthreads();
+  for (int w = NB_TPB / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      better(smax[threadIdx.x], skey[threadIdx.x], smax[threadIdx.x + w], skey[threadIdx.x + w]);
+      ssum[threadIdx.x] += ssum[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x + 0] = smax[0];
+    part[3 * blockIdx.x + 1] = (double)skey[0];
+    part[3 * blockIdx.x + 2] = ssum[0];
+    __threadfence();  // the partial is visible device-wide before the ticket
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  vmax = 0.0;
+  vsum = 0.0;
+  vkey = 0x7fffffffffffffffLL;
+  for (int i = threadIdx.x; i < nb; i += NB_TPB) {
+    // other blocks wrote these: read through L2, past this SM's L1
+    better(vmax, vkey, __ldcg(part + 3 * i), (long long)__ldcg(part + 3 * i + 1));
+    vsum += __ldcg(part + 3 * i + 2);
+  }
+  smax[threadIdx.x] = vmax;
+  skey[threadIdx.x] = vkey;
+  ssum[threadIdx.x] = vsum;
+  __syncthreads();
+  for (int w = NB_TPB / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      better(smax[threadIdx.x], skey[threadIdx.x], smax[threadIdx.x + w], skey[threadIdx.x + w]);
+      ssum[threadIdx.x] += ssum[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    res[0] = smax[0];
+    res[1] = smax[0] > 0.0 ? (double)skey[0] : 0.0;
+    res[2] = sqrt(ssum[0] / (1.0 * P.nx * P.ny * P.nz));
+    *ticket = 0u;
+  }
+}
+
+}  // namespace
+
+int launch_norms_noalloc(const Dev& P, double E, const double* u, double* scratch, int nb, cudaStream_t st) {
+  k_norms_noalloc<<<nb, NB_TPB, 0, st>>>(P, E, u, scratch);
+  return 1;
+}
+
 }  // namespace mts

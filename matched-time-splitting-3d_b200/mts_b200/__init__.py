@@ -159,6 +159,18 @@ class Solver:
         check(self._L.mts_norms(self._h, ctypes.byref(lmax), ctypes.byref(l2), am.ctypes.data), "mts_norms")
         return lmax.value, l2.value, tuple(int(v) for v in am)
 
+    def norms_noalloc(self, u_dev_ptr: int | None = None, t: float = 0.0):
+        """The same norms with no allocation (mts_norms_noalloc): of the
+        device field at address u_dev_ptr evaluated at time t, or of the
+        solver's own solution when u_dev_ptr is None.  Grids of at most
+        4194304 nodes."""
+        lmax, l2 = ctypes.c_double(), ctypes.c_double()
+        am = np.zeros(3, dtype=np.int32)
+        ptr = ctypes.c_void_p(u_dev_ptr) if u_dev_ptr else None
+        check(self._L.mts_norms_noalloc(self._h, ptr, float(t), ctypes.byref(lmax), ctypes.byref(l2),
+                                        am.ctypes.data), "mts_norms_noalloc")
+        return lmax.value, l2.value, tuple(int(v) for v in am)
+
     # -- introspection -------------------------------------------------------
     def counts(self) -> dict:
         c = np.zeros(8, dtype=np.int64)

@@ -40,6 +40,7 @@ EXPORTS = [
     "mts_advance",
     "mts_advance_host",
     "mts_norms",
+    "mts_norms_noalloc",
     "mts_get_time",
     "mts_set_time",
     "mts_synchronize",
@@ -156,6 +157,7 @@ def load(build_if_missing: bool = True):
             "mts_advance": [H, ctypes.c_int32],
             "mts_advance_host": [H, vp, vp, ctypes.c_int32],
             "mts_norms": [H, P(ctypes.c_double), P(ctypes.c_double), vp],
+            "mts_norms_noalloc": [H, vp, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_get_time": [H, P(ctypes.c_double)],
             "mts_set_time": [H, ctypes.c_double],
             "mts_synchronize": [H],
