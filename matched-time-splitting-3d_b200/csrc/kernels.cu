@@ -291,11 +291,31 @@ __global__ void __launch_bounds__(TPB) k_adi_rhs(const Dev P, const double* __re
       R[m] = outer_u(P, E, ix, iy, iz);
       continue;
     }
+    // every load of a regular node issued up front, ahead of the tag test
     const uint8_t tg = P.tag[m];
+    const double uc = un[m], uym = un[m - sy], uyp = un[m + sy], uzm = un[m - sz], uzp = un[m + sz];
     const int side = tg & TAG_OUT;
     const double dt = P.dt;
     const double* vdy = P.vd[1][side];
     const double* vdz = P.vd[2][side];
+    if (!(tg & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
+      double sum = 0.0;
+      sum += uym * vdy[0];
+      sum += uc * vdy[1];
+      sum += uyp * vdy[2];
+      const double ydt = dt * sum;
+      sum = 0.0;
+      sum += uzm * vdz[0];
+      sum += uc * vdz[1];
+      sum += uzp * vdz[2];
+      const double zdt = dt * sum;
+      const double src = source(P, E, side, ix, iy, iz);
+      double r = ydt + zdt;
+      r += uc;
+      r += dt * src;
+      R[m] = r;
+      continue;
+    }
     const MibBlock* xb = nullptr;
     const MibBlock* yb = nullptr;
     const MibBlock* zb = nullptr;
@@ -349,8 +369,18 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit(const Dev P, const double* 
       out[m] = outer_u(P, eh, ix, iy, iz);
       continue;
     }
+    // the loads of a regular node issued up front, ahead of the tag test
     const uint8_t tg = P.tag[m];
+    const double um = in[m - s], uc = in[m], up = in[m + s];
     const double* vd = P.vd[D][tg & TAG_OUT];
+    if (!(tg & flag)) {
+      double sum = 0.0;
+      sum += um * vd[0];
+      sum += uc * vd[1];
+      sum += up * vd[2];
+      out[m] = P.kex * sum + uc;
+      continue;
+    }
     const MibBlock* b = nullptr;
     int r = 0;
     if (tg & flag) b = D == 0 ? find_block<0>(P, iy * P.nz + iz, ix, r) : find_block<1>(P, ix * P.nz + iz, iy, r);
@@ -923,7 +953,9 @@ unsigned pointwise_blocks(const Dev& P) {
 
 // Sweep shapes (rows per chunk, ring chunks, threads per CTA), selected per
 // sweep of a step by Dev::shape (mts_set_sweep_shape / mts_autotune).
-#define MTS_SHAPES(X) X(0, 8, 8, 128) X(1, 4, 16, 128) X(2, 4, 8, 256) X(3, 8, 4, 256) X(4, 4, 8, 192) X(5, 4, 8, 288)
+#define MTS_SHAPES(X)                                                                        \
+  X(0, 8, 8, 128) X(1, 4, 16, 128) X(2, 4, 8, 256) X(3, 8, 4, 256) X(4, 4, 8, 192) X(5, 4, 8, 288) \
+  X(6, 4, 4, 384) X(7, 4, 4, 512) X(8, 4, 4, 448)
 
 template <int D, int KIND, int CH, int NS, int NT>
 void sweep_shape(const Dev& P, const SweepIO& io, cudaStream_t st) {
@@ -957,7 +989,7 @@ void set_smem_attr() {
 
 }  // namespace
 
-int sweep_shape_count() { return 6; }
+int sweep_shape_count() { return 9; }
 
 bool sweep_shape_fits(int shape, int nmax) {
   switch (shape) {
@@ -970,7 +1002,7 @@ bool sweep_shape_fits(int shape, int nmax) {
       return false;
   }
 }
-int sweep_shape_max_threads() { return 288; }
+int sweep_shape_max_threads() { return 512; }
 
 void configure_kernels() {
   set_smem_attr<0, K_COPY>();

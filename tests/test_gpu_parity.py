@@ -108,3 +108,34 @@ def test_gpu_matches_oracle_65(method, surface):
     lo, l2o, amo = O.port_norms(prob, tags, t, u_or)
     assert lmax == lo and tuple(am) == amo
     assert abs(l2 - l2o) <= 1e-12 * l2o
+
+
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+def test_every_sweep_shape_gives_the_oracle_bits(method):
+    """Every compiled sweep shape (chunk rows, ring depth, threads per CTA)
+    takes different fast and slow paths through a line; all must give the
+    oracle's bits.  Line lengths 67/61/70 are not multiples of the chunk rows,
+    so every line ends inside a partial chunk."""
+    n = (67, 61, 70)
+    spec = M.Spec(n=n, surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, method=method,
+                  mib=2, dt=2.0 / 64)
+    tags, cr, _ = M.setup_host(spec)
+    prob = O.Problem(n=n, surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, method=method,
+                     mib=2, dt=2.0 / 64, steps=2)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    tried = 0
+    with M.Solver(spec) as s:
+        for shape in range(M.load().mts_sweep_shape_count()):
+            try:
+                for k in range(3):
+                    s.set_sweep_shape(k, shape)
+            except M.MtsError:
+                continue  # needs more shared memory than these lines allow
+            s.time = 0.0
+            s.initialize()
+            s.advance(2)
+            s.synchronize()
+            u = s.solution()
+            assert np.array_equal(u, u_or), f"shape {shape}: rel {rel_maxdiff(u, u_or):.3e}"
+            tried += 1
+    assert tried >= 6
