@@ -481,6 +481,17 @@ mts_status finish_create(mts_problem* h) {
   uint8_t* dtag = nullptr;
   CUDA_TRY(h->put(&dtag, tag8.data(), tag8.size()));
   D.tag = dtag;
+  {
+    // nodes that are a MIB row of some block: the pointwise passes leave them
+    // to a per-node pass over this list
+    std::vector<long long> mibn;
+    for (long long m = 0; m < N; m++)
+      if (tag8[(size_t)m] & (mts::TAG_MIBX | mts::TAG_MIBY | mts::TAG_MIBZ)) mibn.push_back(m);
+    long long* dm = nullptr;
+    CUDA_TRY(h->put(&dm, mibn.empty() ? nullptr : mibn.data(), mibn.size()));
+    D.mibnode = dm;
+    D.nmibnode = (int)mibn.size();
+  }
   for (int d = 0; d < 3; d++) {
     uint8_t* ls = nullptr;
     CUDA_TRY(h->put(&ls, lside[d].data(), lside[d].size()));

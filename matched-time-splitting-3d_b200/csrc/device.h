@@ -99,6 +99,8 @@ struct Dev {
   double* dp;        // [nmax][sweep threads of the launch]: forward results d'_j
   int sweep_blocks;  // one persistent CTA per SM
   int shape[3];      // sweep shape of the first, second and third sweep of a step
+  const long long* mibnode;  // nodes with a MIB flag (any direction), ascending
+  int nmibnode;
   int* status;       // reserved
 };
 

@@ -283,118 +283,248 @@ __device__ __forceinline__ const MibBlock* find_block(const Dev& P, int lid, int
     for (int ix = threadIdx.x & 31, iy = row_ % (P).ny, iz = row_ / (P).ny; ix < (P).nx; ix += 32) \
       if (long long m = ix + (long long)(P).nx * row_; true)
 
-__global__ void __launch_bounds__(TPB) k_adi_rhs(const Dev P, const double* __restrict__ un,
+// Rows of the pointwise passes: a warp takes one x-row (iy, iz) at a time and
+// covers it in groups of G x 32 nodes (ROW_G, or 2 for the five-load ADI RHS).  All loads of a group are issued
+// before any of them is used, so each warp keeps G rows' worth of DRAM reads
+// in flight; the exact-solution parts fixed along the row are computed once.
+constexpr int ROW_G = 4;
+
+struct RowExact {
+  double y2, z2;   // y*y, z*z
+  double c2y, s2z; // cos 2y, sin 2z
+};
+__device__ __forceinline__ RowExact row_exact(const Dev& P, int iy, int iz) {
+  const double y = P.ax[1][iy], z = P.ax[2][iz];
+  return {y * y, z * z, P.c2[1][iy], P.s2[2][iz]};
+}
+// outer_u and source in the operand order of outer_u / inner_u / source
+__device__ __forceinline__ double row_outer(const Dev& P, const RowExact& q, int ix, double E) {
+  if (P.eq == 0) return 100.0;
+  const double x = P.ax[0][ix];
+  return ((x * x + q.y2) + q.z2) * E;
+}
+__device__ __forceinline__ double row_source(const Dev& P, const RowExact& q, int ix, double E, int out) {
+  if (P.eq == 0) return 0.0;
+  if (out) return -row_outer(P, q, ix, E) - P.c6bo * E;
+  return P.kin * (((P.s2[0][ix] * q.c2y) * q.s2z) * E);
+}
+
+// RHS1 of a node that is a MIB row of some x, y or z block: the general form.
+__device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __restrict__ un, double E, long long m, int ix,
+                                           int iy, int iz, int tg) {
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const int side = tg & TAG_OUT;
+  const double dt = P.dt;
+  const double* vdy = P.vd[1][side];
+  const double* vdz = P.vd[2][side];
+  const MibBlock* xb = nullptr;
+  const MibBlock* yb = nullptr;
+  const MibBlock* zb = nullptr;
+  int xr = 0, yr = 0, zr = 0;
+  double sum, ydt, zdt;
+  if (tg & TAG_MIBY) yb = find_block<1>(P, ix * P.nz + iz, iy, yr);
+  if (yb) {
+    const long long base = ix + sz * iz;
+    sum = mib_sum(*yb, yr, [&](int j) { return un[base + (long long)j * sy]; }, vdy, false, P.jv);
+    ydt = sum * dt;
+  } else {
+    sum = 0.0;
+    sum += un[m - sy] * vdy[0];
+    sum += un[m] * vdy[1];
+    sum += un[m + sy] * vdy[2];
+    ydt = dt * sum;
+  }
+  if (tg & TAG_MIBZ) zb = find_block<2>(P, ix * P.ny + iy, iz, zr);
+  if (zb) {
+    const long long base = ix + (long long)P.nx * iy;
+    sum = mib_sum(*zb, zr, [&](int j) { return un[base + (long long)j * sz]; }, vdz, false, P.jv);
+    zdt = sum * dt;
+  } else {
+    sum = 0.0;
+    sum += un[m - sz] * vdz[0];
+    sum += un[m] * vdz[1];
+    sum += un[m + sz] * vdz[2];
+    zdt = dt * sum;
+  }
+  double src = source(P, E, side, ix, iy, iz);
+  if (tg & TAG_MIBX) xb = find_block<0>(P, iy * P.nz + iz, ix, xr);
+  if (xb) src = adi_src_add(src, *xb, xr, P.vd[0][side], P.jv);
+  if (yb) src = adi_src_add(src, *yb, yr, vdy, P.jv);
+  if (zb) src = adi_src_add(src, *zb, zr, vdz, P.jv);
+  double r = ydt + zdt;
+  r += un[m];
+  r += dt * src;
+  return r;
+}
+
+template <int G>
+__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
                                                  double* __restrict__ R, double E) {
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
-  FOR_EACH_NODE(P) {
-    if (ix == 0 || iy == 0 || iz == 0 || ix == P.nx - 1 || iy == P.ny - 1 || iz == P.nz - 1) {
-      R[m] = outer_u(P, E, ix, iy, iz);
+  const int lane = threadIdx.x & 31;
+  const int nrows = P.ny * P.nz;
+  const double dt = P.dt;
+  // regular 3-point weights by side, in registers
+  const double y0i = P.vd[1][0][0], y1i = P.vd[1][0][1], y2i = P.vd[1][0][2];
+  const double y0o = P.vd[1][1][0], y1o = P.vd[1][1][1], y2o = P.vd[1][1][2];
+  const double z0i = P.vd[2][0][0], z1i = P.vd[2][0][1], z2i = P.vd[2][0][2];
+  const double z0o = P.vd[2][1][0], z1o = P.vd[2][1][1], z2o = P.vd[2][1][2];
+  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+    const int iy = row % P.ny, iz = row / P.ny;
+    const long long m0 = (long long)P.nx * row;
+    const RowExact q = row_exact(P, iy, iz);
+    if (iy == 0 || iz == 0 || iy == P.ny - 1 || iz == P.nz - 1) {
+      for (int ix = lane; ix < P.nx; ix += 32) R[m0 + ix] = row_outer(P, q, ix, E);
       continue;
     }
-    // every load of a regular node issued up front, ahead of the tag test
-    const uint8_t tg = P.tag[m];
-    const double uc = un[m], uym = un[m - sy], uyp = un[m + sy], uzm = un[m - sz], uzp = un[m + sz];
-    const int side = tg & TAG_OUT;
-    const double dt = P.dt;
-    const double* vdy = P.vd[1][side];
-    const double* vdz = P.vd[2][side];
-    if (!(tg & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
-      double sum = 0.0;
-      sum += uym * vdy[0];
-      sum += uc * vdy[1];
-      sum += uyp * vdy[2];
-      const double ydt = dt * sum;
-      sum = 0.0;
-      sum += uzm * vdz[0];
-      sum += uc * vdz[1];
-      sum += uzp * vdz[2];
-      const double zdt = dt * sum;
-      const double src = source(P, E, side, ix, iy, iz);
-      double r = ydt + zdt;
-      r += uc;
-      r += dt * src;
-      R[m] = r;
-      continue;
+    for (int ix0 = 0; ix0 < P.nx; ix0 += 32 * G) {
+      double uc[G], uym[G], uyp[G], uzm[G], uzp[G];
+      int tg[G];
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix < P.nx) {
+          const long long m = m0 + ix;
+          tg[g] = P.tag[m];
+          uc[g] = un[m];
+          uym[g] = un[m - sy];
+          uyp[g] = un[m + sy];
+          uzm[g] = un[m - sz];
+          uzp[g] = un[m + sz];
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix >= P.nx) break;
+        const long long m = m0 + ix;
+        double r;
+        if (ix == 0 || ix == P.nx - 1) {
+          r = row_outer(P, q, ix, E);
+        } else if (!(tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
+          const int side = tg[g] & TAG_OUT;
+          double sum = 0.0;
+          sum += uym[g] * (side ? y0o : y0i);
+          sum += uc[g] * (side ? y1o : y1i);
+          sum += uyp[g] * (side ? y2o : y2i);
+          const double ydt = dt * sum;
+          sum = 0.0;
+          sum += uzm[g] * (side ? z0o : z0i);
+          sum += uc[g] * (side ? z1o : z1i);
+          sum += uzp[g] * (side ? z2o : z2i);
+          const double zdt = dt * sum;
+          const double src = row_source(P, q, ix, E, side);
+          r = ydt + zdt;
+          r += uc[g];
+          r += dt * src;
+        } else {
+          continue;  // a MIB row: k_adi_rhs_mib writes it
+        }
+        R[m] = r;
+      }
     }
-    const MibBlock* xb = nullptr;
-    const MibBlock* yb = nullptr;
-    const MibBlock* zb = nullptr;
-    int xr = 0, yr = 0, zr = 0;
-    double sum, ydt, zdt;
-    if (tg & TAG_MIBY) yb = find_block<1>(P, ix * P.nz + iz, iy, yr);
-    if (yb) {
-      const long long base = ix + sz * iz;
-      sum = mib_sum(*yb, yr, [&](int j) { return un[base + (long long)j * sy]; }, vdy, false, P.jv);
-      ydt = sum * dt;
-    } else {
-      sum = 0.0;
-      sum += un[m - sy] * vdy[0];
-      sum += un[m] * vdy[1];
-      sum += un[m + sy] * vdy[2];
-      ydt = dt * sum;
-    }
-    if (tg & TAG_MIBZ) zb = find_block<2>(P, ix * P.ny + iy, iz, zr);
-    if (zb) {
-      const long long base = ix + (long long)P.nx * iy;
-      sum = mib_sum(*zb, zr, [&](int j) { return un[base + (long long)j * sz]; }, vdz, false, P.jv);
-      zdt = sum * dt;
-    } else {
-      sum = 0.0;
-      sum += un[m - sz] * vdz[0];
-      sum += un[m] * vdz[1];
-      sum += un[m + sz] * vdz[2];
-      zdt = dt * sum;
-    }
-    double src = source(P, E, side, ix, iy, iz);
-    if (tg & TAG_MIBX) xb = find_block<0>(P, iy * P.nz + iz, ix, xr);
-    if (xb) src = adi_src_add(src, *xb, xr, P.vd[0][side], P.jv);
-    if (yb) src = adi_src_add(src, *yb, yr, vdy, P.jv);
-    if (zb) src = adi_src_add(src, *zb, zr, vdz, P.jv);
-    double r = ydt + zdt;
-    r += un[m];
-    r += dt * src;
-    R[m] = r;
   }
+}
+
+// The MIB rows of RHS1, one thread per listed node.
+__global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                     double* __restrict__ R, double E) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= P.nmibnode) return;
+  const long long m = P.mibnode[k];
+  int ix, iy, iz;
+  node_xyz(P, m, ix, iy, iz);
+  R[m] = adi_rhs_mib(P, un, E, m, ix, iy, iz, P.tag[m]);
 }
 
 // TS explicit half step along D = x or y (TS::D_xx_r / D_yy_r, the LOD
 // Crank-Nicolson operators, trapezoidal.cc:319-895), then Set_bc at t_half.
 template <int D>
-__global__ void __launch_bounds__(TPB) k_ts_explicit(const Dev P, const double* __restrict__ in,
+__device__ __forceinline__ double ts_explicit_mib(const Dev& P, const double* __restrict__ in, long long m, int ix,
+                                               int iy, int iz, int tg) {
+  const long long s = D == 0 ? 1 : (long long)P.nx;
+  const double* vd = P.vd[D][tg & TAG_OUT];
+  int r = 0;
+  const MibBlock* b = D == 0 ? find_block<0>(P, iy * P.nz + iz, ix, r) : find_block<1>(P, ix * P.nz + iz, iy, r);
+  double sum;
+  if (b) {
+    const long long base = D == 0 ? m - ix : m - (long long)iy * P.nx;
+    sum = mib_sum(*b, r, [&](int j) { return in[base + (long long)j * s]; }, vd, true, P.jv);
+  } else {
+    sum = 0.0;
+    sum += in[m - s] * vd[0];
+    sum += in[m] * vd[1];
+    sum += in[m + s] * vd[2];
+  }
+  return P.kex * sum + in[m];
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__ Dev P, const double* __restrict__ in,
+                                                         double* __restrict__ out) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= P.nmibnode) return;
+  const long long m = P.mibnode[k];
+  const int tg = P.tag[m];
+  if (!(tg & (D == 0 ? TAG_MIBX : TAG_MIBY))) return;
+  int ix, iy, iz;
+  node_xyz(P, m, ix, iy, iz);
+  out[m] = ts_explicit_mib<D>(P, in, m, ix, iy, iz, tg);
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in,
                                                      double* __restrict__ out, double eh) {
   const long long s = D == 0 ? 1 : (long long)P.nx;
-  const uint8_t flag = D == 0 ? TAG_MIBX : TAG_MIBY;
-  FOR_EACH_NODE(P) {
-    if (ix == 0 || iy == 0 || iz == 0 || ix == P.nx - 1 || iy == P.ny - 1 || iz == P.nz - 1) {
-      out[m] = outer_u(P, eh, ix, iy, iz);
+  const int flag = D == 0 ? TAG_MIBX : TAG_MIBY;
+  const int lane = threadIdx.x & 31;
+  const int nrows = P.ny * P.nz;
+  const double kex = P.kex;
+  const double w0i = P.vd[D][0][0], w1i = P.vd[D][0][1], w2i = P.vd[D][0][2];
+  const double w0o = P.vd[D][1][0], w1o = P.vd[D][1][1], w2o = P.vd[D][1][2];
+  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+    const int iy = row % P.ny, iz = row / P.ny;
+    const long long m0 = (long long)P.nx * row;
+    const RowExact q = row_exact(P, iy, iz);
+    if (iy == 0 || iz == 0 || iy == P.ny - 1 || iz == P.nz - 1) {
+      for (int ix = lane; ix < P.nx; ix += 32) out[m0 + ix] = row_outer(P, q, ix, eh);
       continue;
     }
-    // the loads of a regular node issued up front, ahead of the tag test
-    const uint8_t tg = P.tag[m];
-    const double um = in[m - s], uc = in[m], up = in[m + s];
-    const double* vd = P.vd[D][tg & TAG_OUT];
-    if (!(tg & flag)) {
-      double sum = 0.0;
-      sum += um * vd[0];
-      sum += uc * vd[1];
-      sum += up * vd[2];
-      out[m] = P.kex * sum + uc;
-      continue;
+    for (int ix0 = 0; ix0 < P.nx; ix0 += 32 * ROW_G) {
+      double um[ROW_G], uc[ROW_G], up[ROW_G];
+      int tg[ROW_G];
+#pragma unroll
+      for (int g = 0; g < ROW_G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix < P.nx) {
+          const long long m = m0 + ix;
+          tg[g] = P.tag[m];
+          uc[g] = in[m];
+          um[g] = in[m - s];
+          up[g] = in[m + s];
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < ROW_G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix >= P.nx) break;
+        const long long m = m0 + ix;
+        double v;
+        if (ix == 0 || ix == P.nx - 1) {
+          v = row_outer(P, q, ix, eh);
+        } else if (!(tg[g] & flag)) {
+          const int side = tg[g] & TAG_OUT;
+          double sum = 0.0;
+          sum += um[g] * (side ? w0o : w0i);
+          sum += uc[g] * (side ? w1o : w1i);
+          sum += up[g] * (side ? w2o : w2i);
+          v = kex * sum + uc[g];
+        } else {
+          continue;  // a MIB row of a D block: k_ts_explicit_mib writes it
+        }
+        out[m] = v;
+      }
     }
-    const MibBlock* b = nullptr;
-    int r = 0;
-    if (tg & flag) b = D == 0 ? find_block<0>(P, iy * P.nz + iz, ix, r) : find_block<1>(P, ix * P.nz + iz, iy, r);
-    double sum;
-    if (b) {
-      const long long base = D == 0 ? m - ix : m - (long long)iy * P.nx;
-      sum = mib_sum(*b, r, [&](int j) { return in[base + (long long)j * s]; }, vd, true, P.jv);
-    } else {
-      sum = 0.0;
-      sum += in[m - s] * vd[0];
-      sum += in[m] * vd[1];
-      sum += in[m + s] * vd[2];
-    }
-    out[m] = P.kex * sum + in[m];
   }
 }
 
@@ -1055,7 +1185,11 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
     // builds uhss = -dt D_yy u^n + u* and solves in place (u**); z sweep builds
     // uh1 = -dt D_zz u^n + u** and solves in place (u^{n+1}).
     mark(0);
-    k_adi_rhs<<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_next);
+    k_adi_rhs<2><<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_next);
+    if (P.nmibnode > 0) {
+      k_adi_rhs_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u0, u1, T.e_next);
+      launches++;
+    }
     mark(1);
     io.stin = u1;
     io.add = u1;
@@ -1111,9 +1245,17 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
     // z + sources + implicit z in place on u0, then implicit y and x in place.
     mark(0);
     k_ts_explicit<0><<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_half);
+    if (P.nmibnode > 0) {
+      k_ts_explicit_mib<0><<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u0, u1);
+      launches++;
+    }
     mark(1);
     mark(0);
     k_ts_explicit<1><<<pointwise_blocks(P), TPB, 0, st>>>(P, u1, u0, T.e_half);
+    if (P.nmibnode > 0) {
+      k_ts_explicit_mib<1><<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u1, u0);
+      launches++;
+    }
     mark(1);
     io.jumps = 1;
     io.k = P.kex;
