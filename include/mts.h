@@ -204,6 +204,19 @@ int32_t mts_sweep_shape_count(void);
 mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape);
 mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
 
+/* Arithmetic of the step.  MTS_PRECISION_PLAIN (the default) is the FP64
+ * drop-in, bit-identical to the reference.  MTS_PRECISION_MIXED (Douglas-ADI
+ * only) solves each step for its increment u^{n+1} - u^n: the residual
+ * dt (A_x + A_y + A_z) u^n + dt src is formed in FP64, the three line solves
+ * of douglas_adi.cc:66-1110 run on the FP32 increment with FP32 factors, and
+ * the increment is added to the FP64 state.  Results differ from the plain
+ * form by the FP32 rounding of one step's increment per step; the error
+ * against the exact solution stays that of the plain form.  No counterpart
+ * in the reference, which computes in FP64 only. */
+typedef enum { MTS_PRECISION_PLAIN = 0, MTS_PRECISION_MIXED = 1 } mts_precision;
+mts_status mts_set_precision(mts_handle h, int32_t precision);
+mts_status mts_get_precision(mts_handle h, int32_t* precision);
+
 /* Text of the last error on this thread. */
 const char* mts_last_error(void);
 

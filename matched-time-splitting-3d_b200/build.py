@@ -19,8 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmts_b200.so")
-SOURCES = ["setup.cpp", "kernels.cu", "capi.cu"]
-HEADERS = ["setup.h", "device.h"]
+SOURCES = ["setup.cpp", "kernels.cu", "mixed.cu", "capi.cu"]
+HEADERS = ["setup.h", "device.h", "device_common.cuh"]
+OBJ_DIR = os.path.join(HERE, "build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -48,19 +49,32 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    flags = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O3",
+             "-Xptxas", "-O3"]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        cp = subprocess.run(cmd, capture_output=True, text=True)
+        if cp.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src} ({cp.returncode}):\n{cp.stdout}\n{cp.stderr}")
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
     tmp = LIB + ".tmp"
-    cmd = [
-        nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-fmad=false",
-        "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-Xptxas", "-O3",
-        "-shared", "-o", tmp, *[os.path.join(CSRC, s) for s in SOURCES],
-        "-lcudart",
-    ]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     cp = subprocess.run(cmd, capture_output=True, text=True)
     if cp.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({cp.returncode}):\n{cp.stdout}\n{cp.stderr}")
+        raise RuntimeError(f"link failed ({cp.returncode}):\n{cp.stdout}\n{cp.stderr}")
     os.replace(tmp, LIB)
     return LIB
 

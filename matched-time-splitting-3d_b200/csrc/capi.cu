@@ -439,6 +439,7 @@ mts_status finish_create(mts_problem* h) {
   static bool configured = false;
   if (!configured) {
     mts::configure_kernels();
+    mts::configure_mixed_kernels();
     configured = true;
   }
   int sms = 0;
@@ -477,6 +478,38 @@ mts_status finish_create(mts_problem* h) {
     }
     D.fbet[d] = fb;
     D.fgam[d] = fg;
+    // the same factors in FP32 for the mixed-precision sweeps, as 1/bet and gam
+    for (int side = 0; side < 2; side++) {
+      std::vector<float> p32(ptab[d][side].size());
+      for (size_t j = 0; j + 1 < p32.size(); j += 2) {
+        p32[j] = (float)(1.0 / ptab[d][side][j]);
+        p32[j + 1] = (float)ptab[d][side][j + 1];
+      }
+      float* pt = nullptr;
+      CUDA_TRY(h->put(&pt, p32.data(), p32.size()));
+      D.ptab32[d][side] = pt;
+    }
+    float *fb32 = nullptr, *fg32 = nullptr;
+    if (!fbet[d].empty()) {
+      std::vector<float> v((size_t)N);
+      for (size_t m = 0; m < v.size(); m++) v[m] = fbet[d][m] != 0.0 ? (float)(1.0 / fbet[d][m]) : 0.0f;
+      CUDA_TRY(h->put_padded(&fb32, v.data(), v.size(), fpad));
+      for (size_t m = 0; m < v.size(); m++) v[m] = (float)fgam[d][m];
+      CUDA_TRY(h->put_padded(&fg32, v.data(), v.size(), fpad));
+      // the host copies must outlive the asynchronous uploads
+      CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    D.fib32[d] = fb32;
+    D.fgam32[d] = fg32;
+    float* rb32 = nullptr;
+    CUDA_TRY(h->put(&rb32, (const float*)nullptr, 3 * blocks[d].size()));
+    D.rblk32[d] = rb32;
+  }
+  {
+    const size_t t32 = (size_t)D.sweep_blocks * (size_t)mts::mixed_sweep_threads();
+    CUDA_TRY(h->put_padded(&D.r32, (const float*)nullptr, (size_t)N, fpad));
+    CUDA_TRY(h->put_padded(&D.dp32, (const float*)nullptr, (size_t)nmax * t32, (size_t)mts::kRowPad * t32));
+    D.precision = 0;
   }
   uint8_t* dtag = nullptr;
   CUDA_TRY(h->put(&dtag, tag8.data(), tag8.size()));
@@ -567,7 +600,10 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
     h->ev_free.pop_back();
     ev = h->ev_busy.back().data();
   }
-  h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev);
+  if (h->dev.precision == 1)
+    h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev);
+  else
+    h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MTS_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
   h->t = t_next;
@@ -885,6 +921,25 @@ mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape) {
   if (!mts::sweep_shape_fits(shape, std::max(h->g.nx, std::max(h->g.ny, h->g.nz))))
     return fail(MTS_ERR_ARG, "shape needs more shared memory than this grid allows");
   h->dev.shape[sweep] = shape;
+  return MTS_OK;
+}
+
+mts_status mts_set_precision(mts_handle h, int32_t precision) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  if (precision != MTS_PRECISION_PLAIN && precision != MTS_PRECISION_MIXED)
+    return fail(MTS_ERR_ARG, "precision must be MTS_PRECISION_PLAIN or MTS_PRECISION_MIXED");
+  if (precision == MTS_PRECISION_MIXED) {
+    if (h->prm.method != MTS_ADI) return fail(MTS_ERR_ARG, "the mixed-precision form is built for Douglas-ADI only");
+    if (!mts::mixed_shape_fits(std::max(h->g.nx, std::max(h->g.ny, h->g.nz))))
+      return fail(MTS_ERR_ARG, "grid lines too long for the mixed-precision sweeps' shared memory");
+  }
+  h->dev.precision = precision;
+  return MTS_OK;
+}
+
+mts_status mts_get_precision(mts_handle h, int32_t* precision) {
+  if (!h || !precision) return fail(MTS_ERR_ARG, "null argument");
+  *precision = h->dev.precision;
   return MTS_OK;
 }
 

@@ -99,6 +99,16 @@ struct Dev {
   double* dp;        // [nmax][sweep threads of the launch]: forward results d'_j
   int sweep_blocks;  // one persistent CTA per SM
   int shape[3];      // sweep shape of the first, second and third sweep of a step
+  // Mixed precision (Douglas-ADI): the step is solved for its increment
+  // delta = u^{n+1} - u^n in FP32 (residual in FP64, state accumulated in
+  // FP64).  Factors as 1/bet and gam in FP32, laid out like ptab/fbet/fgam.
+  float* r32;                 // residual in, increment out [N + slack]
+  float* dp32;                // [nmax + slack][sweep threads]
+  const float* ptab32[3][2];  // [2*j + {0: 1/bet, 1: gam}]
+  const float* fib32[3];      // per node 1/bet of crossing lines from L1
+  const float* fgam32[3];
+  float* rblk32[3];           // block rows' right-hand sides after Convert2Tri
+  int precision;              // 0 plain FP64, 1 mixed
   const long long* mibnode;  // nodes with a MIB flag (any direction), ascending
   int nmibnode;
   int* status;       // reserved
@@ -122,6 +132,14 @@ int launch_initialize(const Dev& P, double E, double* u, cudaStream_t stream);
 // ev: null, or 2 events per kernel slot recorded around each launch.
 int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t stream,
                 cudaEvent_t* ev);
+// The mixed-precision Douglas-ADI step (mixed.cu), in place on u.
+int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t stream, cudaEvent_t* ev);
+void configure_mixed_kernels();
+int mixed_sweep_threads();            // threads per CTA of the FP32 sweeps
+bool mixed_shape_fits(int nmax);      // their shared memory within the limit
+// Shared by both step forms (kernels.cu).
+void launch_jumps(const Dev& P, double E, cudaStream_t stream);
+unsigned pointwise_rows_grid(const Dev& P);
 constexpr int kProfileSlots = 8;
 constexpr int kRowPad = 16;  // rows of slack after each staged field (>= chunk rows)
 int launch_norms(const Dev& P, double E, const double* u, double* partial, int nblocks,

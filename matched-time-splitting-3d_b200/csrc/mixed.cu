@@ -1,0 +1,476 @@
+// Mixed-precision form of the Douglas-ADI step (precision = 1).
+//
+// The Douglas step (douglas_adi.cc:66-1110) is three line solves,
+//   (I - A_x) u*     = u^n + A_y u^n + A_z u^n + dt src
+//   (I - A_y) u**    = u* - A_y u^n
+//   (I - A_z) u^n+1  = u** - A_z u^n,
+// with A_d = dt beta D_dd (MIB rows included) and src carrying f and the jump
+// terms of Src_2nd.  Written for the increments d* = u* - u^n, d** = u** - u^n
+// and d = u^{n+1} - u^n the same equations read
+//   (I - A_x) d*  = rho = dt (A_x u^n + A_y u^n + A_z u^n + src)
+//   (I - A_y) d** = d*
+//   (I - A_z) d   = d**,      u^{n+1} = u^n + d,
+// and on the faces d = Outer_u(t^{n+1}) - u^n.  The residual rho is formed in
+// FP64 from the FP64 state, the three line solves run on FP32 increments
+// (4-byte fields and scratch, FP32 factors), and the increment is added to the
+// FP64 state inside the last sweep.  The FP32 rounding thus touches only the
+// increment of one step, never the accumulated solution.
+#include <cuda_runtime.h>
+
+#include "device.h"
+#include "device_common.cuh"
+
+namespace mts {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Residual rho = dt (A_x u + A_y u + A_z u + src), FP64 in, FP32 out.
+
+template <int G>
+__global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                   float* __restrict__ rho, double E) {
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const int lane = threadIdx.x & 31;
+  const int nrows = P.ny * P.nz;
+  const double dt = P.dt;
+  const double x0i = P.vd[0][0][0], x1i = P.vd[0][0][1], x2i = P.vd[0][0][2];
+  const double x0o = P.vd[0][1][0], x1o = P.vd[0][1][1], x2o = P.vd[0][1][2];
+  const double y0i = P.vd[1][0][0], y1i = P.vd[1][0][1], y2i = P.vd[1][0][2];
+  const double y0o = P.vd[1][1][0], y1o = P.vd[1][1][1], y2o = P.vd[1][1][2];
+  const double z0i = P.vd[2][0][0], z1i = P.vd[2][0][1], z2i = P.vd[2][0][2];
+  const double z0o = P.vd[2][1][0], z1o = P.vd[2][1][1], z2o = P.vd[2][1][2];
+  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+    const int iy = row % P.ny, iz = row / P.ny;
+    const long long m0 = (long long)P.nx * row;
+    const RowExact q = row_exact(P, iy, iz);
+    if (iy == 0 || iz == 0 || iy == P.ny - 1 || iz == P.nz - 1) {
+      for (int ix = lane; ix < P.nx; ix += 32) rho[m0 + ix] = (float)(row_outer(P, q, ix, E) - un[m0 + ix]);
+      continue;
+    }
+    for (int ix0 = 0; ix0 < P.nx; ix0 += 32 * G) {
+      double uc[G], uxm[G], uxp[G], uym[G], uyp[G], uzm[G], uzp[G];
+      int tg[G];
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix < P.nx) {
+          // interior row: m0 - 1 and m0 + nx are inside the field
+          const long long m = m0 + ix;
+          tg[g] = P.tag[m];
+          uc[g] = un[m];
+          uxm[g] = un[m - 1];
+          uxp[g] = un[m + 1];
+          uym[g] = un[m - sy];
+          uyp[g] = un[m + sy];
+          uzm[g] = un[m - sz];
+          uzp[g] = un[m + sz];
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        const int ix = ix0 + 32 * g + lane;
+        if (ix >= P.nx) break;
+        const long long m = m0 + ix;
+        double r;
+        if (ix == 0 || ix == P.nx - 1) {
+          r = row_outer(P, q, ix, E) - uc[g];
+        } else if (!(tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
+          const int side = tg[g] & TAG_OUT;
+          const double sx = (uxm[g] * (side ? x0o : x0i) + uc[g] * (side ? x1o : x1i)) + uxp[g] * (side ? x2o : x2i);
+          const double sy_ = (uym[g] * (side ? y0o : y0i) + uc[g] * (side ? y1o : y1i)) + uyp[g] * (side ? y2o : y2i);
+          const double sz_ = (uzm[g] * (side ? z0o : z0i) + uc[g] * (side ? z1o : z1i)) + uzp[g] * (side ? z2o : z2i);
+          r = dt * (((sx + sy_) + sz_) + row_source(P, q, ix, E, side));
+        } else {
+          continue;  // a MIB row: k_adi_resid_mib writes it
+        }
+        rho[m] = (float)r;
+      }
+    }
+  }
+}
+
+// The MIB rows of rho, one thread per listed node: the explicit MIB sums of
+// every direction the node is a MIB row of (douglas_adi.cc:112-210, without
+// jumps) and the jump terms of Src_2nd (douglas_adi.cc:1156-1427).
+__global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                       float* __restrict__ rho, double E) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= P.nmibnode) return;
+  const long long m = P.mibnode[k];
+  int ix, iy, iz;
+  node_xyz(P, m, ix, iy, iz);
+  const int tg = P.tag[m];
+  const int side = tg & TAG_OUT;
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double* vdx = P.vd[0][side];
+  const double* vdy = P.vd[1][side];
+  const double* vdz = P.vd[2][side];
+  int xr = 0, yr = 0, zr = 0;
+  const MibBlock* xb = (tg & TAG_MIBX) ? find_block<0>(P, iy * P.nz + iz, ix, xr) : nullptr;
+  const MibBlock* yb = (tg & TAG_MIBY) ? find_block<1>(P, ix * P.nz + iz, iy, yr) : nullptr;
+  const MibBlock* zb = (tg & TAG_MIBZ) ? find_block<2>(P, ix * P.ny + iy, iz, zr) : nullptr;
+  double sx, sy_, sz_;
+  if (xb) {
+    const long long base = m - ix;
+    sx = mib_sum(*xb, xr, [&](int j) { return un[base + j]; }, vdx, false, P.jv);
+  } else {
+    sx = (un[m - 1] * vdx[0] + un[m] * vdx[1]) + un[m + 1] * vdx[2];
+  }
+  if (yb) {
+    const long long base = ix + sz * iz;
+    sy_ = mib_sum(*yb, yr, [&](int j) { return un[base + (long long)j * sy]; }, vdy, false, P.jv);
+  } else {
+    sy_ = (un[m - sy] * vdy[0] + un[m] * vdy[1]) + un[m + sy] * vdy[2];
+  }
+  if (zb) {
+    const long long base = ix + (long long)P.nx * iy;
+    sz_ = mib_sum(*zb, zr, [&](int j) { return un[base + (long long)j * sz]; }, vdz, false, P.jv);
+  } else {
+    sz_ = (un[m - sz] * vdz[0] + un[m] * vdz[1]) + un[m + sz] * vdz[2];
+  }
+  double src = source(P, E, side, ix, iy, iz);
+  if (xb) src = adi_src_add(src, *xb, xr, vdx, P.jv);
+  if (yb) src = adi_src_add(src, *yb, yr, vdy, P.jv);
+  if (zb) src = adi_src_add(src, *zb, zr, vdz, P.jv);
+  rho[m] = (float)(P.dt * (((sx + sy_) + sz_) + src));
+}
+
+// ---------------------------------------------------------------------------
+// FP32 line solves of the increments.
+
+// Block pre-pass: the Convert2Tri row operations (douglas_adi.cc:1554-1675)
+// on the right-hand sides of each block's rows, in FP64, stored in FP32.
+template <int D>
+__global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev P, const float* __restrict__ f,
+                                                     int nblk) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= nblk) return;
+  const MibBlock& b = P.blk[D][k];
+  const int n2 = D == 2 ? P.ny : P.nz;
+  Line L;
+  decode_line<D>(P, (long long)(b.line % n2) * (D == 0 ? P.ny : P.nx) + b.line / n2, L);
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < b.kind; q++) r[q] = f[L.base + (long long)(b.L + q) * L.s];
+  if (b.kind == 2) {
+    r[1] -= b.rate[0] * r[0];
+    r[0] -= b.rate[1] * r[1];
+  } else {
+    r[1] -= b.rate[0] * r[0];
+    r[2] -= b.rate[1] * r[0];
+    r[0] -= b.rate[2] * r[2];
+    r[1] -= b.rate[3] * r[2];
+    r[2] -= b.rate[4] * r[1];
+    r[0] -= b.rate[5] * r[1];
+  }
+  for (int q = 0; q < 3; q++) P.rblk32[D][3 * k + q] = (float)r[q];
+}
+
+struct BlockHead32 {
+  int L, kind, sides;
+  float a0, a1, a2;  // sub-diagonal of the block's rows after Convert2Tri
+  float r0, r1, r2;  // their right-hand sides this sweep
+};
+
+__device__ __forceinline__ void load_head32(const MibBlock* blk, const float* rblk, int k, int end, BlockHead32& h) {
+  if (k < end) {
+    const MibBlock& b = blk[k];
+    h.L = b.L;
+    h.kind = b.kind;
+    h.sides = b.sides;
+    h.a0 = (float)b.ia[0];
+    h.a1 = (float)b.ia[1];
+    h.a2 = (float)b.ia[2];
+    h.r0 = rblk[3 * k];
+    h.r1 = rblk[3 * k + 1];
+    h.r2 = rblk[3 * k + 2];
+  } else {
+    h.L = 0x7fffffff;
+    h.kind = 0;
+    h.sides = 0;
+  }
+}
+
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+template <int CH, int NS, int NT>
+constexpr size_t shape32_smem(int n) {
+  return sizeof(float) * ((size_t)2 * NS * CH * NT + (size_t)4 * n);
+}
+
+// One thread per line, persistent CTAs, as the FP64 sweep (kernels.cu): f
+// holds the right-hand side and receives the increment in place; with ACC the
+// increment is added to the FP64 state u instead.  Ring A stages f (forward)
+// and d' (backward); ring C stages 1/bet (forward) and gam (backward) of
+// crossing lines from their first MIB row on.
+template <int D, bool ACC, int CH, int NS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P, float* f, double* __restrict__ u) {
+  static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4 && CH <= kRowPad, "shape");
+  constexpr int RING = NS * CH;
+  constexpr int SLOT = CH * NT;
+  extern __shared__ float sm32[];
+  const int tid = threadIdx.x;
+  float* const sA = sm32 + tid;
+  float* const sC = sA + NS * SLOT;
+#define RA(j) sA[((j) & (RING - 1)) * NT]
+#define RC(j) sC[((j) & (RING - 1)) * NT]
+  const long long T = (long long)gridDim.x * NT;
+  const long long gt = (long long)blockIdx.x * NT + tid;
+  float* const dp = P.dp32 + gt;
+  const long long nl = nlines<D>(P);
+  const MibBlock* __restrict__ blk = P.blk[D];
+  const float* __restrict__ fib = P.fib32[D];
+  const float* __restrict__ fgam = P.fgam32[D];
+  const float* __restrict__ rblk = P.rblk32[D];
+  const float ai = (float)P.ia[D][0], ao = (float)P.ia[D][1];
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  float* const sP = sm32 + 2 * NS * SLOT;
+  for (int i = tid; i < 4 * nd; i += NT) sP[i] = i < 2 * nd ? P.ptab32[D][0][i] : P.ptab32[D][1][i - 2 * nd];
+  __syncthreads();
+
+  for (long long t = gt; t < nl; t += T) {
+    Line L;
+    decode_line<D>(P, t, L);
+    const int n = L.n;
+    const long long s = L.s;
+    if (L.boundary) {
+      // face line: the increment is the right-hand side itself
+      if (ACC)
+        for (int j = 0; j < n; j++) {
+          const long long m = L.base + (long long)j * s;
+          u[m] = u[m] + (double)f[m];
+        }
+      continue;
+    }
+    const int nch = (n + CH - 1) / CH;
+    const int ls = P.lside[D][L.lid];
+    const int bfirst = P.bstart[D][L.lid];
+    const int bend = P.bstart[D][L.lid + 1];
+    const int L1 = bfirst < bend ? blk[bfirst].L : n;
+    const float* pt = sP + ((ls >> 1) & 1) * 2 * nd;
+    const float* gA = f + L.base;
+    const float* gC = fib + L.base;
+    auto stage = [&](int c) {
+      if (c < nch) {
+        const long long off = (long long)c * CH * s;
+        float* a = sA + (c & (NS - 1)) * SLOT;
+#pragma unroll
+        for (int r = 0; r < CH; r++) cp_async4(a + r * NT, gA + off + r * s);
+        if ((c + 1) * CH > L1) {
+          float* cc = sC + (c & (NS - 1)) * SLOT;
+#pragma unroll
+          for (int r = 0; r < CH; r++) cp_async4(cc + r * NT, gC + off + r * s);
+        }
+      }
+      cp_async_commit();
+    };
+
+    // forward: d'_j = (r_j - a_j d'_{j-1}) / bet_j
+    for (int c = 0; c < NS - 2; c++) stage(c);
+    int mb = bfirst;
+    BlockHead32 hb, hb2;
+    load_head32(blk, rblk, mb, bend, hb);
+    load_head32(blk, rblk, mb + 1, bend, hb2);
+    int mside = (ls >> 1) & 1;
+    float dprev = 0.0f;
+    int j = 1;
+    for (int c = 0; c < nch; c++) {
+      stage(c + NS - 2);
+      cp_async_wait<NS - 3>();
+      if (c == 0) {
+        dprev = RA(0) * pt[0];
+        dp[0] = dprev;
+      }
+      const int c0 = c * CH;
+      const int cend = min(c0 + CH, n - 1);
+      if (j >= cend) continue;
+      if (j == c0 && cend == c0 + CH && hb.L >= cend && (cend <= L1 || c0 >= L1)) {
+        const float ac = mside ? ao : ai;
+        const float* a = sA + (c & (NS - 1)) * SLOT;
+        float* q = dp + (long long)c0 * T;
+        auto run = [&](auto tag) {
+          constexpr bool kField = decltype(tag)::value;
+          const float* bt = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0;
+#pragma unroll
+          for (int rr = 0; rr < CH; rr++) {
+            const float ib = kField ? bt[rr * NT] : bt[2 * rr];
+            const float d = __fmul_rn(__fmaf_rn(-ac, dprev, a[rr * NT]), ib);
+            q[rr * T] = d;
+            dprev = d;
+          }
+        };
+        if (c0 >= L1)
+          run(BoolC<true>{});
+        else
+          run(BoolC<false>{});
+        j = cend;
+      } else {
+        while (j < cend) {
+          const float ib = j >= L1 ? RC(j) : pt[2 * j];
+          if (j == hb.L) {
+            float d = __fmul_rn(__fmaf_rn(-hb.a0, dprev, hb.r0), ib);
+            dp[(long long)j * T] = d;
+            d = __fmul_rn(__fmaf_rn(-hb.a1, d, hb.r1), RC(j + 1));
+            dp[(long long)(j + 1) * T] = d;
+            if (hb.kind == 3) {
+              d = __fmul_rn(__fmaf_rn(-hb.a2, d, hb.r2), RC(j + 2));
+              dp[(long long)(j + 2) * T] = d;
+            }
+            dprev = d;
+            mside = (hb.sides >> (hb.kind - 1)) & 1;
+            j += hb.kind;
+            mb++;
+            hb = hb2;
+            load_head32(blk, rblk, mb + 1, bend, hb2);
+          } else {
+            const float d = __fmul_rn(__fmaf_rn(-(mside ? ao : ai), dprev, RA(j)), ib);
+            dp[(long long)j * T] = d;
+            dprev = d;
+            j++;
+          }
+        }
+      }
+    }
+    {
+      // last row: the Dirichlet identity row (a = 0)
+      const float ib = n - 1 >= L1 ? RC(n - 1) : pt[2 * (n - 1)];
+      dp[(long long)(n - 1) * T] = __fmul_rn(RA(n - 1), ib);
+    }
+    cp_async_wait<0>();
+
+    // backward: x_j = d'_j - gam_{j+1} x_{j+1}
+    __threadfence_block();
+    const float* gG = fgam + L.base;
+    auto bstage = [&](int c) {
+      if (c >= 0) {
+        float* a = sA + (c & (NS - 1)) * SLOT;
+        const float* g = dp + (long long)c * CH * T;
+#pragma unroll
+        for (int r = 0; r < CH; r++) cp_async4(a + r * NT, g + r * T);
+        if ((c + 1) * CH >= L1) {
+          float* b = sC + (c & (NS - 1)) * SLOT;
+          const long long off = ((long long)c * CH + 1) * s;
+#pragma unroll
+          for (int r = 0; r < CH; r++) cp_async4(b + r * NT, gG + off + r * s);
+        }
+      }
+      cp_async_commit();
+    };
+    float xnext = 0.0f;
+    for (int c = nch - 1; c > nch - NS; c--) bstage(c);
+    for (int c = nch - 1; c >= 0; c--) {
+      bstage(c - NS + 1);
+      cp_async_wait<NS - 1>();
+      const int c0 = c * CH;
+      if (c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
+        const float* a = sA + (c & (NS - 1)) * SLOT;
+        double uo[CH];
+        if (ACC) {
+#pragma unroll
+          for (int rr = 0; rr < CH; rr++) uo[rr] = u[L.base + (long long)(c0 + rr) * s];
+        }
+        auto run = [&](auto tag) {
+          constexpr bool kField = decltype(tag)::value;
+          const float* gb = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0 + 3;
+#pragma unroll
+          for (int rr = CH - 1; rr >= 0; rr--) {
+            const float gm = kField ? gb[rr * NT] : gb[2 * rr];
+            const float x = __fmaf_rn(-gm, xnext, a[rr * NT]);
+            xnext = x;
+            const long long m = L.base + (long long)(c0 + rr) * s;
+            if (ACC)
+              u[m] = uo[rr] + (double)x;
+            else
+              f[m] = x;
+          }
+        };
+        if (c0 + 1 >= L1)
+          run(BoolC<true>{});
+        else
+          run(BoolC<false>{});
+      } else {
+        for (int rr = CH - 1; rr >= 0; rr--) {
+          const int jj = c0 + rr;
+          if (jj >= n) continue;
+          float x = RA(jj);
+          if (jj != n - 1) x = __fmaf_rn(-(jj + 1 >= L1 ? RC(jj) : pt[2 * (jj + 1) + 1]), xnext, x);
+          xnext = x;
+          const long long m = L.base + (long long)jj * s;
+          if (ACC)
+            u[m] = u[m] + (double)x;
+          else
+            f[m] = x;
+        }
+      }
+    }
+    cp_async_wait<0>();
+  }
+#undef RA
+#undef RC
+}
+
+// Shapes of the FP32 sweep (rows per chunk, ring chunks, threads per CTA).
+constexpr int S32_CH = 8, S32_NS = 4, S32_NT = 448;
+
+template <int D, bool ACC>
+void sweep32(const Dev& P, float* f, double* u, cudaStream_t st) {
+  if (P.nblk[D] > 0) k_block_rhs32<D><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  k_sweep32<D, ACC, S32_CH, S32_NS, S32_NT>
+      <<<P.sweep_blocks, S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f, u);
+}
+
+}  // namespace
+
+void configure_mixed_kernels() {
+  constexpr int smem = 232448;
+  cudaFuncSetAttribute(k_sweep32<0, false, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       smem);
+  cudaFuncSetAttribute(k_sweep32<1, false, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       smem);
+  cudaFuncSetAttribute(k_sweep32<2, true, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       smem);
+}
+
+int mixed_sweep_threads() { return S32_NT; }
+
+bool mixed_shape_fits(int nmax) { return shape32_smem<S32_CH, S32_NS, S32_NT>(nmax) <= (size_t)232448; }
+
+int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t st, cudaEvent_t* ev) {
+  int launches = 0;
+  int slot = 0;
+  auto mark = [&](int k) {
+    if (ev) cudaEventRecord(ev[2 * slot + k], st);
+    if (k == 1) slot++;
+  };
+  mark(0);
+  if (P.ncross > 0) {
+    launch_jumps(P, T.e_next, st);
+    launches++;
+  }
+  mark(1);
+  mark(0);
+  k_adi_resid<2><<<pointwise_rows_grid(P), TPB, 0, st>>>(P, u, P.r32, T.e_next);
+  launches++;
+  if (P.nmibnode > 0) {
+    k_adi_resid_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u, P.r32, T.e_next);
+    launches++;
+  }
+  mark(1);
+  mark(0);
+  sweep32<0, false>(P, P.r32, u, st);
+  mark(1);
+  mark(0);
+  sweep32<1, false>(P, P.r32, u, st);
+  mark(1);
+  mark(0);
+  sweep32<2, true>(P, P.r32, u, st);
+  mark(1);
+  launches += 3;
+  for (int d = 0; d < 3; d++) launches += P.nblk[d] > 0;
+  return launches;
+}
+
+}  // namespace mts

@@ -209,6 +209,20 @@ class Solver:
     def set_sweep_shape(self, sweep: int, shape: int) -> None:
         check(self._L.mts_set_sweep_shape(self._h, int(sweep), int(shape)), "mts_set_sweep_shape")
 
+    PRECISIONS = {"plain": 0, "mixed": 1}
+
+    def set_precision(self, precision: str) -> None:
+        """"plain" (FP64, bit-identical to the reference) or "mixed" (FP32
+        line solves on the step's increment, FP64 residual and state;
+        Douglas-ADI only)."""
+        check(self._L.mts_set_precision(self._h, self.PRECISIONS[precision]), "mts_set_precision")
+
+    @property
+    def precision(self) -> str:
+        v = ctypes.c_int32()
+        check(self._L.mts_get_precision(self._h, ctypes.byref(v)), "mts_get_precision")
+        return {0: "plain", 1: "mixed"}[v.value]
+
     def autotune(self, steps: int = 2):
         """Times every compiled sweep shape on this problem and keeps the
         fastest per sweep; the solution and time are left unchanged."""

@@ -54,6 +54,8 @@ EXPORTS = [
     "mts_sweep_shape_count",
     "mts_set_sweep_shape",
     "mts_autotune",
+    "mts_set_precision",
+    "mts_get_precision",
     "mts_last_error",
     "mts_version",
 ]
@@ -170,6 +172,8 @@ def load(build_if_missing: bool = True):
             "mts_profile_read": [H, vp, vp],
             "mts_set_sweep_shape": [H, ctypes.c_int32, ctypes.c_int32],
             "mts_autotune": [H, ctypes.c_int32, vp],
+            "mts_set_precision": [H, ctypes.c_int32],
+            "mts_get_precision": [H, P(ctypes.c_int32)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -1,0 +1,63 @@
+"""The mixed-precision form of the Douglas-ADI step against the plain FP64
+form (itself bit-identical to the reference).
+
+The mixed form solves each step for its increment in FP32, with the residual
+and the state in FP64, so it differs from the plain form by the FP32 rounding
+of the increments.  Tolerances, written here:
+  * relative max-norm difference from the plain solution <= 2e-5 after 8
+    steps (a few ulp of FP32 per step on an O(dt) increment);
+  * L-infinity error against the exact solution within 1.05x of the plain
+    form's (the accuracy contract of the mixed form)."""
+import numpy as np
+import pytest
+
+import mts_b200 as M
+from conftest import rel_maxdiff
+
+pytestmark = pytest.mark.gpu
+REL_TOL = 2e-5
+LINF_RATIO = 1.05
+
+
+def run(spec, precision, steps):
+    with M.Solver(spec) as s:
+        s.set_precision(precision)
+        assert s.precision == precision
+        s.initialize()
+        s.advance(steps)
+        s.synchronize()
+        return s.solution(), s.norms()
+
+
+@pytest.mark.parametrize("surface,mib", [("torus", 2), ("torus", 1), ("ellipsoid", 2), ("ellipsoid", 1)])
+def test_mixed_matches_plain(surface, mib):
+    sp = (0.5, 0.2) if surface == "torus" else (0.7001, 0.4999, 0.4001, 1.0)
+    spec = M.Spec(n=(65, 65, 65), surface=surface, surface_params=sp, beta_in=1.0, beta_out=1000.0, method="adi",
+                  mib=mib, dt=2.0 / 64)
+    u_p, (l_p, l2_p, _) = run(spec, "plain", 8)
+    u_m, (l_m, l2_m, _) = run(spec, "mixed", 8)
+    d = rel_maxdiff(u_m, u_p)
+    assert d <= REL_TOL, f"relative max-norm difference {d:.3e}"
+    assert l_m <= LINF_RATIO * l_p and l_p <= LINF_RATIO * l_m, (l_m, l_p)
+    assert abs(l2_m - l2_p) <= 0.05 * l2_p
+
+
+@pytest.mark.parametrize("beta_out", [1e-3, 1.0, 1e3])
+def test_mixed_beta_ratios_anisotropic(beta_out):
+    """The precision config's beta ratios, on an anisotropic grid with line
+    lengths that are not multiples of the sweep chunk."""
+    spec = M.Spec(n=(67, 61, 70), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=beta_out,
+                  method="adi", mib=2, dt=2.0 / 64)
+    u_p, (l_p, _, _) = run(spec, "plain", 6)
+    u_m, (l_m, _, _) = run(spec, "mixed", 6)
+    assert rel_maxdiff(u_m, u_p) <= REL_TOL
+    assert l_m <= LINF_RATIO * l_p
+
+
+def test_mixed_rejects_other_methods():
+    spec = M.Spec(n=(33, 33, 33), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=10.0,
+                  method="lod-cn", mib=2, dt=1.0 / 16)
+    with M.Solver(spec) as s:
+        with pytest.raises(M.MtsError, match="Douglas-ADI only"):
+            s.set_precision("mixed")
+        assert s.precision == "plain"
