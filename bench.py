@@ -34,6 +34,20 @@ WORKLOAD = dict(n=(257, 257, 257), surface="torus", surface_params=(0.5, 0.2), b
                 method="adi", mib=2, dt=2.0 / 256)
 METRIC = "cell-steps/s @256^3 plain FP64"
 REF_MAX_STEPS = 3  # timed steps per reference process (CPU arm)
+# Algorithmic bytes per node and step of the mixed ADI form: residual (read
+# u^n 8 + tag 1, write rho 4), x, y and z FP32 solves (4 + 4 each), and the
+# accumulation pass (read 4, read u^n 8, write u^{n+1} 8).
+MIXED_BYTES = 13 + 8 + 8 + 8 + 20
+CONTRACT_BYTES = {"adi": 67, "lod-ie": 51, "lod-cn": 51, "ts": 102}
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def peak_hbm() -> float:
+    """Measured copy bandwidth of this pool's B200s (GB/s), else the fallback."""
+    if os.path.exists(PEAKS_PATH):
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"])
+    return 6650.0
 
 # Algorithmic HBM bytes per grid node per launch of each kernel slot
 # (field reads/writes at 8 B plus the 1-byte node tag; scratch excluded).
@@ -64,6 +78,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: auto)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default sweep shapes")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run (ADI only)")
     ap.add_argument("--shapes", default="", help="sweep shapes of the three sweeps, e.g. 4,4,4 (no autotune)")
     return ap.parse_args()
 
@@ -299,6 +314,8 @@ def main():
     solver.set_profiling(False)
     launches = solver.launch_count() - launches0
     lmax, l2, _ = solver.norms()
+    t_plain = solver.time
+    u_plain = solver.solution() if (w["method"] == "adi" and not a.no_mixed) else None
 
     # end to end through the C ABI with host buffers: the field goes up and
     # comes back every step (the reference's Solve_2nd contract on a host
@@ -325,6 +342,56 @@ def main():
     value = world * nodes * a.steps / (ms_max / 1e3)
     e2e_value = world * nodes * e2e_steps / (e2e_max / 1e3)
 
+    # The mixed-precision form (FP32 line solves on the increment, FP64
+    # residual and state) on the same workload, same steps from the same
+    # start, so its error is compared at the same time.
+    mixed = None
+    if u_plain is not None:
+        sm = M.Solver(spec)
+        sm.set_precision("mixed")
+        sm.initialize()
+        sm.advance(a.warmup)
+        sm.synchronize()
+        stream_m = torch.cuda.ExternalStream(sm.stream())
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        sm.set_profiling(True)
+        sm.profile_read()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        m0.record(stream_m)
+        sm.advance(a.steps)
+        m1.record(stream_m)
+        sm.synchronize()
+        ms_m = m0.elapsed_time(m1)
+        kms_m, kn_m = sm.profile_read()
+        sm.set_profiling(False)
+        lm, l2m, _ = sm.norms()
+        um = sm.solution()
+        rel = float(abs(um - u_plain).max() / max(1e-300, abs(u_plain).max()))
+        assert sm.time == t_plain
+        sm.close()
+        del um
+        tm = torch.tensor([ms_m], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ms_m = float(tm[0])
+        v_m = world * nodes * a.steps / (ms_m / 1e3)
+        names_m = ["jumps", "residual_fp64", "x_sweep_fp32", "y_sweep_fp32", "z_sweep_fp32_and_accumulate"]
+        mixed = {
+            "value": v_m, "unit": "cell-steps/s", "ms_per_step": ms_m / a.steps,
+            "speedup_vs_plain": v_m / (world * nodes * a.steps / (ms / 1e3)),
+            "lmax": lm, "l2": l2m, "lmax_plain": lmax, "l2_plain": l2, "lmax_ratio": lm / lmax,
+            "rel_maxdiff_vs_plain": rel, "t": t_plain,
+            "bytes_per_node_step": MIXED_BYTES,
+            "step_roofline_frac": MIXED_BYTES * nodes * a.steps / (ms_m / 1e3) / 1e9 / peak_hbm(),
+            "kernels": {n: {"ms_per_launch": kms_m[k] / kn_m[k], "launches": int(kn_m[k])}
+                        for k, n in enumerate(names_m) if kn_m[k] > 0},
+            "form": "residual dt(A_x+A_y+A_z)u^n + dt src in FP64, three FP32 line solves of the increment, "
+                    "FP64 state += increment after the z sweep",
+        }
+
     method = w["method"]
     names = SLOT_NAMES[method]
     kernels = {}
@@ -333,12 +400,7 @@ def main():
             kernels[name] = {"ms_per_launch": kms[k] / kn[k], "launches": int(kn[k]),
                              "share": kms[k] / max(1e-12, kms[: len(names)].sum())}
     dom = max((k for k in ALG_BYTES[method]), key=lambda k: kms[k])
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak, peak_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        with open(peaks_path) as f:
-            peak = float(json.load(f)["hbm_gbs"])
-        peak_src = "measured"
+    peak, peak_src = peak_hbm(), ("measured" if os.path.exists(PEAKS_PATH) else "fallback")
     per_launch_ms = kms[dom] / kn[dom]
     achieved = ALG_BYTES[method][dom] * nodes / (per_launch_ms / 1e3) / 1e9
     step_bytes = sum(ALG_BYTES[method].values())
@@ -347,6 +409,10 @@ def main():
         "frac": achieved / peak, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})",
         "traffic": None,
         "algorithmic_bytes_per_node": ALG_BYTES[method][dom],
+        # the contract's step model counts the first RHS fused into the x
+        # sweep: 67 B per node-step for ADI (51 LOD, 102 TS)
+        "step_contract": {"bytes_per_node_step": CONTRACT_BYTES[method],
+                          "frac": CONTRACT_BYTES[method] * nodes * a.steps / (ms / 1e3) / 1e9 / peak},
         "step": {"bytes_per_node_step": step_bytes,
                  "achieved": step_bytes * nodes * a.steps / (ms / 1e3) / 1e9,
                  "frac": step_bytes * nodes * a.steps / (ms / 1e3) / 1e9 / peak},
@@ -368,8 +434,10 @@ def main():
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * nodes,
                 "d2h_bytes_per_step": 8 * nodes, "steps": e2e_steps,
                 "api": "mts_advance_host (field uploaded and downloaded every step, pinned host memory)"},
-        "clocks": clk, "accuracy": {"lmax": lmax, "l2": l2, "t": solver.time},
+        "clocks": clk, "accuracy": {"lmax": lmax, "l2": l2, "t": t_plain},
     }
+    if mixed is not None:
+        line["mixed"] = mixed
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             res = run_reference_sample(w, a.ref_procs or auto_procs(w), 1)

@@ -13,7 +13,7 @@
 // and on the faces d = Outer_u(t^{n+1}) - u^n.  The residual rho is formed in
 // FP64 from the FP64 state, the three line solves run on FP32 increments
 // (4-byte fields and scratch, FP32 factors), and the increment is added to the
-// FP64 state inside the last sweep.  The FP32 rounding thus touches only the
+// FP64 state after the last sweep.  The FP32 rounding thus touches only the
 // increment of one step, never the accumulated solution.
 #include <cuda_runtime.h>
 
@@ -195,18 +195,19 @@ __device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
+// Shared memory of a shape: rings A and C and the two prefix factor tables
+// (2 sides x 2 values x n rows), all FP32.
 template <int CH, int NS, int NT>
 constexpr size_t shape32_smem(int n) {
   return sizeof(float) * ((size_t)2 * NS * CH * NT + (size_t)4 * n);
 }
 
 // One thread per line, persistent CTAs, as the FP64 sweep (kernels.cu): f
-// holds the right-hand side and receives the increment in place; with ACC the
-// increment is added to the FP64 state u instead.  Ring A stages f (forward)
-// and d' (backward); ring C stages 1/bet (forward) and gam (backward) of
-// crossing lines from their first MIB row on.
-template <int D, bool ACC, int CH, int NS, int NT>
-__global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P, float* f, double* __restrict__ u) {
+// holds the right-hand side and receives the solution in place.  Ring A
+// stages f (forward) and d' (backward); ring C stages 1/bet (forward) and gam
+// (backward) of crossing lines from their first MIB row on.
+template <int D, int CH, int NS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P, float* f) {
   static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4 && CH <= kRowPad, "shape");
   constexpr int RING = NS * CH;
   constexpr int SLOT = CH * NT;
@@ -235,15 +236,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
     decode_line<D>(P, t, L);
     const int n = L.n;
     const long long s = L.s;
-    if (L.boundary) {
-      // face line: the increment is the right-hand side itself
-      if (ACC)
-        for (int j = 0; j < n; j++) {
-          const long long m = L.base + (long long)j * s;
-          u[m] = u[m] + (double)f[m];
-        }
-      continue;
-    }
+    if (L.boundary) continue;  // face line: the solution is the right-hand side itself
     const int nch = (n + CH - 1) / CH;
     const int ls = P.lside[D][L.lid];
     const int bfirst = P.bstart[D][L.lid];
@@ -366,11 +359,6 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
       const int c0 = c * CH;
       if (c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
         const float* a = sA + (c & (NS - 1)) * SLOT;
-        double uo[CH];
-        if (ACC) {
-#pragma unroll
-          for (int rr = 0; rr < CH; rr++) uo[rr] = u[L.base + (long long)(c0 + rr) * s];
-        }
         auto run = [&](auto tag) {
           constexpr bool kField = decltype(tag)::value;
           const float* gb = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0 + 3;
@@ -379,11 +367,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
             const float gm = kField ? gb[rr * NT] : gb[2 * rr];
             const float x = __fmaf_rn(-gm, xnext, a[rr * NT]);
             xnext = x;
-            const long long m = L.base + (long long)(c0 + rr) * s;
-            if (ACC)
-              u[m] = uo[rr] + (double)x;
-            else
-              f[m] = x;
+            f[L.base + (long long)(c0 + rr) * s] = x;
           }
         };
         if (c0 + 1 >= L1)
@@ -397,11 +381,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
           float x = RA(jj);
           if (jj != n - 1) x = __fmaf_rn(-(jj + 1 >= L1 ? RC(jj) : pt[2 * (jj + 1) + 1]), xnext, x);
           xnext = x;
-          const long long m = L.base + (long long)jj * s;
-          if (ACC)
-            u[m] = u[m] + (double)x;
-          else
-            f[m] = x;
+          f[L.base + (long long)jj * s] = x;
         }
       }
     }
@@ -412,26 +392,43 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
 }
 
 // Shapes of the FP32 sweep (rows per chunk, ring chunks, threads per CTA).
+// Shape of the FP32 sweeps (rows per chunk, ring chunks, threads per CTA):
+// 448 threads on each of the 148 SMs cover the 66,049 lines of a 257^3 grid
+// in one wave.
 constexpr int S32_CH = 8, S32_NS = 4, S32_NT = 448;
 
-template <int D, bool ACC>
-void sweep32(const Dev& P, float* f, double* u, cudaStream_t st) {
+template <int D>
+void sweep32(const Dev& P, float* f, cudaStream_t st) {
   if (P.nblk[D] > 0) k_block_rhs32<D><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
   const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
-  k_sweep32<D, ACC, S32_CH, S32_NS, S32_NT>
-      <<<P.sweep_blocks, S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f, u);
+  k_sweep32<D, S32_CH, S32_NS, S32_NT><<<P.sweep_blocks, S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f);
+}
+
+// u^{n+1} = u^n + d, four nodes per thread
+__global__ void __launch_bounds__(256) k_accumulate(double* __restrict__ u, const float* __restrict__ d, long long n) {
+  const long long stride = (long long)gridDim.x * 256;
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n; i += 4 * stride) {
+    double a[4];
+    float b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (i + k * stride < n) {
+        a[k] = u[i + k * stride];
+        b[k] = d[i + k * stride];
+      }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (i + k * stride < n) u[i + k * stride] = a[k] + (double)b[k];
+  }
 }
 
 }  // namespace
 
 void configure_mixed_kernels() {
   constexpr int smem = 232448;
-  cudaFuncSetAttribute(k_sweep32<0, false, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       smem);
-  cudaFuncSetAttribute(k_sweep32<1, false, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       smem);
-  cudaFuncSetAttribute(k_sweep32<2, true, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       smem);
+  cudaFuncSetAttribute(k_sweep32<0, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_sweep32<1, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(k_sweep32<2, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 int mixed_sweep_threads() { return S32_NT; }
@@ -460,15 +457,16 @@ int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t 
   }
   mark(1);
   mark(0);
-  sweep32<0, false>(P, P.r32, u, st);
+  sweep32<0>(P, P.r32, st);
   mark(1);
   mark(0);
-  sweep32<1, false>(P, P.r32, u, st);
+  sweep32<1>(P, P.r32, st);
   mark(1);
   mark(0);
-  sweep32<2, true>(P, P.r32, u, st);
+  sweep32<2>(P, P.r32, st);
+  k_accumulate<<<4 * P.sweep_blocks * 4, 256, 0, st>>>(u, P.r32, P.nn);
   mark(1);
-  launches += 3;
+  launches += 4;
   for (int d = 0; d < 3; d++) launches += P.nblk[d] > 0;
   return launches;
 }
