@@ -126,6 +126,16 @@ mts_status mts_solve_2nd(mts_handle h, double t_prev, double t_half, double t_ne
  * step; TS evaluates at t-dt, t-dt/2, t).  Asynchronous. */
 mts_status mts_advance(mts_handle h, int32_t nsteps);
 
+/* nsteps steps of each of n independent handles, run as one batch: one step
+ * of every handle is captured into a single CUDA graph, whose branches the
+ * device runs concurrently, and the graph is replayed nsteps times (two
+ * steps per graph when a plain Douglas-ADI handle is in the batch).  Each
+ * handle's result and time are those of mts_advance(h, nsteps), bit for bit.
+ * Handles must be distinct, on one device, with profiling off.  Synchronous.
+ * Batches several problems as the reference, which steps one problem per
+ * process (helper.h:199-426), has no counterpart for. */
+mts_status mts_batch_advance(const mts_handle* handles, int32_t n, int32_t nsteps);
+
 /* The same loop with the caller's host field: u_in is uploaded, nsteps steps
  * run, the result is downloaded into u_out (which may equal u_in).  This is
  * the per-call cost of the reference's Solve_2nd(..., CubicDoub& uh, ...)

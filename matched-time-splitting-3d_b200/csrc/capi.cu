@@ -445,12 +445,21 @@ mts_status finish_create(mts_problem* h) {
   int sms = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   D.sweep_blocks = sms > 0 ? sms : 1;
-  const size_t tmax = (size_t)D.sweep_blocks * (size_t)mts::sweep_shape_max_threads();
+  // sweep threads of a launch: one CTA per SM at most and no more CTAs than
+  // the lines of a direction need, so at most max lines + one CTA
+  long long maxlines = 0;
+  for (int d = 0; d < 3; d++) maxlines = std::max(maxlines, (long long)line_count(g, d));
+  const size_t tmax = std::min((size_t)D.sweep_blocks * (size_t)mts::sweep_shape_max_threads(),
+                               (size_t)maxlines + (size_t)mts::sweep_shape_max_threads());
   const int nmax = std::max(g.nx, std::max(g.ny, g.nz));
   {
+    // default shape: the large-CTA shape 3 when the lines fill the GPU, the
+    // small shape 9 (several CTAs per SM, for concurrent small problems) when
+    // they do not; mts_autotune picks per problem
+    const int want = maxlines >= (long long)D.sweep_blocks * 256 ? 3 : 9;
     int def = -1;
     for (int s = mts::sweep_shape_count() - 1; s >= 0; s--)
-      if (mts::sweep_shape_fits(s, nmax) && (def < 0 || s == 3)) def = s;
+      if (mts::sweep_shape_fits(s, nmax) && (def < 0 || s == want)) def = s;
     if (def < 0) return fail(MTS_ERR_ARG, "grid lines too long for the sweep kernels' shared memory");
     for (int k = 0; k < 3; k++) D.shape[k] = def;
   }
@@ -506,7 +515,8 @@ mts_status finish_create(mts_problem* h) {
     D.rblk32[d] = rb32;
   }
   {
-    const size_t t32 = (size_t)D.sweep_blocks * (size_t)mts::mixed_sweep_threads();
+    const size_t t32 = std::min((size_t)D.sweep_blocks * (size_t)mts::mixed_sweep_threads(),
+                                (size_t)maxlines + (size_t)mts::mixed_sweep_threads());
     CUDA_TRY(h->put_padded(&D.r32, (const float*)nullptr, (size_t)N, fpad));
     CUDA_TRY(h->put_padded(&D.dp32, (const float*)nullptr, (size_t)nmax * t32, (size_t)mts::kRowPad * t32));
     D.precision = 0;
@@ -744,6 +754,136 @@ mts_status mts_solve_2nd(mts_handle h, double t_prev, double t_half, double t_ne
 mts_status mts_advance(mts_handle h, int32_t nsteps) {
   if (!h || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
   return advance(h, nsteps);
+}
+
+// Batched stepping.  Each handle keeps its own device state and kernels; one
+// step of every handle is captured into a single CUDA graph (the handles'
+// launches are independent branches that the device runs concurrently) and
+// the graph is replayed.  A replay must not bake in the step's times, so each
+// handle gets a table of its per-step exp(-t) factors, computed here exactly as
+// advance() computes them, and a device step counter that the graph advances;
+// the kernels read the factors from the table.  Plain Douglas-ADI swaps its
+// two fields every step, so graphs hold two steps when such a handle is in
+// the batch.
+mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
+  if (!hs || n < 1 || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
+  for (int i = 0; i < n; i++) {
+    if (!hs[i]) return fail(MTS_ERR_ARG, "null handle in batch");
+    for (int k = 0; k < i; k++)
+      if (hs[k] == hs[i]) return fail(MTS_ERR_ARG, "a handle appears twice in the batch");
+    if (hs[i]->device != hs[0]->device) return fail(MTS_ERR_ARG, "batch handles live on different devices");
+    if (hs[i]->profiling) return fail(MTS_ERR_ARG, "profiling is on for a batch handle");
+  }
+  if (nsteps == 0) return MTS_OK;
+  struct Sched {
+    double* tab = nullptr;
+    int* step = nullptr;
+    double t_end = 0;
+    int64_t graph_launches = 0;
+  };
+  std::vector<Sched> sc((size_t)n);
+  cudaStream_t root = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<cudaEvent_t> evs;
+  mts_status st = MTS_OK;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t e : evs)
+      if (e) cudaEventDestroy(e);
+    if (root) cudaStreamDestroy(root);
+    for (int i = 0; i < n; i++) {
+      hs[i]->dev.tsched = nullptr;
+      hs[i]->dev.tstep = nullptr;
+      if (sc[(size_t)i].tab) cudaFree(sc[(size_t)i].tab);
+      if (sc[(size_t)i].step) cudaFree(sc[(size_t)i].step);
+    }
+  };
+#define BATCH_TRY(call)                                                                          \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      st = fail(e_ == cudaErrorMemoryAllocation ? MTS_ERR_OOM : MTS_ERR_CUDA,                    \
+                std::string(#call) + ": " + cudaGetErrorString(e_));                             \
+      cleanup();                                                                                 \
+      return st;                                                                                 \
+    }                                                                                            \
+  } while (0)
+  bool two = false;
+  for (int i = 0; i < n; i++) {
+    mts_problem* h = hs[i];
+    if (h->prm.method == MTS_ADI && h->dev.precision == 0) two = true;
+    std::vector<double> tab(3 * (size_t)nsteps);
+    double t = h->t;
+    const double dt = h->prm.dt;
+    for (int k = 0; k < nsteps; k++) {
+      const double t1 = t + dt;
+      tab[3 * (size_t)k] = std::exp(-(t1 - dt));
+      tab[3 * (size_t)k + 1] = std::exp(-(t1 - 0.5 * dt));
+      tab[3 * (size_t)k + 2] = std::exp(-t1);
+      t = t1;
+    }
+    sc[(size_t)i].t_end = t;
+    BATCH_TRY(cudaMalloc((void**)&sc[(size_t)i].tab, tab.size() * sizeof(double)));
+    BATCH_TRY(cudaMalloc((void**)&sc[(size_t)i].step, sizeof(int)));
+    BATCH_TRY(cudaMemcpyAsync(sc[(size_t)i].tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                              h->stream));
+    BATCH_TRY(cudaMemsetAsync(sc[(size_t)i].step, 0, sizeof(int), h->stream));
+    BATCH_TRY(cudaStreamSynchronize(h->stream));
+    h->dev.tsched = sc[(size_t)i].tab;
+    h->dev.tstep = sc[(size_t)i].step;
+  }
+  const int g = two ? 2 : 1;
+  auto enqueue = [&](mts_problem* h, int steps) {
+    int64_t c = 0;
+    for (int k = 0; k < steps; k++) {
+      mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
+      if (h->dev.precision == 1)
+        c += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr);
+      else
+        c += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, nullptr);
+      mts::launch_tick(h->dev, h->stream);
+      c++;
+    }
+    return c;
+  };
+  const int replays = nsteps / g;
+  BATCH_TRY(cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking));
+  evs.assign((size_t)n + 2, nullptr);
+  for (auto& e : evs) BATCH_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (replays > 0) {
+    BATCH_TRY(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal));
+    BATCH_TRY(cudaEventRecord(evs[(size_t)n], root));
+    for (int i = 0; i < n; i++) {
+      mts_problem* h = hs[i];
+      BATCH_TRY(cudaStreamWaitEvent(h->stream, evs[(size_t)n], 0));
+      sc[(size_t)i].graph_launches = enqueue(h, g);
+      BATCH_TRY(cudaEventRecord(evs[(size_t)i], h->stream));
+      BATCH_TRY(cudaStreamWaitEvent(root, evs[(size_t)i], 0));
+    }
+    BATCH_TRY(cudaStreamEndCapture(root, &graph));
+    BATCH_TRY(cudaGraphInstantiate(&exec, graph, 0));
+    for (int r = 0; r < replays; r++) BATCH_TRY(cudaGraphLaunch(exec, root));
+    for (int i = 0; i < n; i++) hs[i]->launches += sc[(size_t)i].graph_launches * replays;
+  }
+  // a step left over (odd count with two-step graphs) runs outside the graph
+  BATCH_TRY(cudaEventRecord(evs[(size_t)n + 1], root));
+  for (int i = 0; i < n; i++) {
+    mts_problem* h = hs[i];
+    BATCH_TRY(cudaStreamWaitEvent(h->stream, evs[(size_t)n + 1], 0));
+    h->launches += enqueue(h, nsteps - replays * g);
+  }
+  for (int i = 0; i < n; i++) {
+    mts_problem* h = hs[i];
+    mts_status s2 = sync_status(h);
+    if (s2 && !st) st = s2;
+    h->t = sc[(size_t)i].t_end;
+  }
+  BATCH_TRY(cudaStreamSynchronize(root));
+  cleanup();
+#undef BATCH_TRY
+  return st;
 }
 
 mts_status mts_advance_host(mts_handle h, const double* u_in, double* u_out, int32_t nsteps) {

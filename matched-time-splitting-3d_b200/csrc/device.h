@@ -109,6 +109,11 @@ struct Dev {
   const float* fgam32[3];
   float* rblk32[3];           // block rows' right-hand sides after Convert2Tri
   int precision;              // 0 plain FP64, 1 mixed
+  // Replayable steps (batches captured in a CUDA graph): when tsched is set,
+  // kernels take the step's exp(-t) factors from tsched[3*(*tstep) + {0: t_prev,
+  // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
+  const double* tsched;
+  int* tstep;
   const long long* mibnode;  // nodes with a MIB flag (any direction), ascending
   int nmibnode;
   int* status;       // reserved
@@ -139,6 +144,7 @@ int mixed_sweep_threads();            // threads per CTA of the FP32 sweeps
 bool mixed_shape_fits(int nmax);      // their shared memory within the limit
 // Shared by both step forms (kernels.cu).
 void launch_jumps(const Dev& P, double E, cudaStream_t stream);
+void launch_tick(const Dev& P, cudaStream_t stream);  // ++(*P.tstep)
 unsigned pointwise_rows_grid(const Dev& P);
 constexpr int kProfileSlots = 8;
 constexpr int kRowPad = 16;  // rows of slack after each staged field (>= chunk rows)

@@ -47,6 +47,19 @@ __device__ __forceinline__ double source(const Dev& P, double E, int out, int ix
   return P.kin * inner_u(P, E, ix, iy, iz);
 }
 
+// CTAs of a persistent line sweep: one per SM at most, no more than nl lines
+// of nt threads need.
+inline unsigned sweep_grid(const Dev& P, long long nl, int nt) {
+  const long long b = (nl + nt - 1) / nt;
+  return (unsigned)(b < P.sweep_blocks ? (b > 0 ? b : 1) : P.sweep_blocks);
+}
+
+// The step's time factor k (0: exp(-t_prev), 1: exp(-t_half), 2: exp(-t_next)):
+// the launch argument, or the step table of a replayed graph.
+__device__ __forceinline__ double step_e(const Dev& P, double given, int k) {
+  return P.tsched ? P.tsched[3 * (*P.tstep) + k] : given;
+}
+
 // ---------------------------------------------------------------------------
 // Line geometry.  Direction D lines are indexed (i1, i2) as in the reference
 // (src/constant.h:83-89): x -> (iy, iz), y -> (ix, iz), z -> (ix, iy); the

@@ -99,6 +99,7 @@ __device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __rest
 template <int G>
 __global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
                                                  double* __restrict__ R, double E) {
+  E = step_e(P, E, 2);
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
   const int nrows = P.ny * P.nz;
@@ -170,6 +171,7 @@ __global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev
                                                      double* __restrict__ R, double E) {
   const int k = blockIdx.x * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
+  E = step_e(P, E, 2);
   const long long m = P.mibnode[k];
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
@@ -214,6 +216,7 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__
 template <int D>
 __global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in,
                                                      double* __restrict__ out, double eh) {
+  eh = step_e(P, eh, 1);
   const long long s = D == 0 ? 1 : (long long)P.nx;
   const int flag = D == 0 ? TAG_MIBX : TAG_MIBY;
   const int lane = threadIdx.x & 31;
@@ -323,6 +326,7 @@ __global__ void __launch_bounds__(TPB) k_block_rhs(const Dev P, const SweepIO io
   Line L;
   decode_line<D>(P, (long long)(b.line % n2) * (D == 0 ? P.ny : P.nx) + b.line / n2, L);
   const double* stin = KIND == K_COPY ? io.add : io.stin;
+  const double e0 = step_e(P, io.e0, 0), e1 = step_e(P, io.e1, 2);
   auto U = [&](int j) { return stin[L.base + (long long)j * L.s]; };
   double r[3] = {0.0, 0.0, 0.0};
   for (int q = 0; q < b.kind; q++) {
@@ -337,8 +341,8 @@ __global__ void __launch_bounds__(TPB) k_block_rhs(const Dev P, const SweepIO io
       if (KIND == K_TS_Z) {
         int ix, iy, iz;
         node_of<D>(L, jj, ix, iy, iz);
-        v = v + P.hdt * source(P, io.e0, side, ix, iy, iz);
-        v = v + P.hdt * source(P, io.e1, side, ix, iy, iz);
+        v = v + P.hdt * source(P, e0, side, ix, iy, iz);
+        v = v + P.hdt * source(P, e1, side, ix, iy, iz);
       }
       r[q] = v;
     }
@@ -426,7 +430,8 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
   const double* __restrict__ fbet = P.fbet[D];
   const double* __restrict__ fgam = P.fgam[D];
   const double* __restrict__ rblk = P.rblk[D];
-  const double E1 = io.e1;
+  const double E1 = step_e(P, io.e1, 2);
+  const double E0 = step_e(P, io.e0, 0);
   const double kx = io.k;
   // per-direction constants by side (0 inside, 1 outside), in registers
   const double v0i = P.vd[D][0][0], v0o = P.vd[D][1][0];
@@ -515,7 +520,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
       if (KIND == K_TS_Z) {
         double S, R2;
         row_parts<D>(fx, sX, nd, j, S, R2);
-        r = r + P.hdt * source_from(P, S, R2, io.e0, side);
+        r = r + P.hdt * source_from(P, S, R2, E0, side);
         r = r + P.hdt * source_from(P, S, R2, E1, side);
       }
       return r;
@@ -721,6 +726,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
 __global__ void __launch_bounds__(TPB) k_jumps(const Dev P, double E) {
   int c = blockIdx.x * TPB + threadIdx.x;
   if (c >= P.ncross) return;
+  E = step_e(P, E, 2);
   const CrossConst q = P.cc[c];
   double ju, jb[3];
   if (P.eq == 0) {
@@ -820,12 +826,13 @@ unsigned pointwise_blocks(const Dev& P) {
 // sweep of a step by Dev::shape (mts_set_sweep_shape / mts_autotune).
 #define MTS_SHAPES(X)                                                                        \
   X(0, 8, 8, 128) X(1, 4, 16, 128) X(2, 4, 8, 256) X(3, 8, 4, 256) X(4, 4, 8, 192) X(5, 4, 8, 288) \
-  X(6, 4, 4, 384) X(7, 4, 4, 512) X(8, 4, 4, 448)
+  X(6, 4, 4, 384) X(7, 4, 4, 512) X(8, 4, 4, 448) X(9, 4, 4, 128)
 
 template <int D, int KIND, int CH, int NS, int NT>
 void sweep_shape(const Dev& P, const SweepIO& io, cudaStream_t st) {
+  // persistent CTAs, one per SM at most, no more than the lines need
   const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
-  k_sweep<D, KIND, CH, NS, NT><<<P.sweep_blocks, NT, shape_smem<CH, NS, NT>(nd), st>>>(P, io);
+  k_sweep<D, KIND, CH, NS, NT><<<sweep_grid(P, nlines<D>(P), NT), NT, shape_smem<CH, NS, NT>(nd), st>>>(P, io);
 }
 
 template <int D, int KIND>
@@ -854,7 +861,7 @@ void set_smem_attr() {
 
 }  // namespace
 
-int sweep_shape_count() { return 9; }
+int sweep_shape_count() { return 10; }
 
 bool sweep_shape_fits(int shape, int nmax) {
   switch (shape) {
@@ -878,6 +885,10 @@ void configure_kernels() {
   set_smem_attr<2, K_STENCIL>();
   set_smem_attr<2, K_TS_Z>();
 }
+
+__global__ void k_tick(int* step) { ++*step; }
+
+void launch_tick(const Dev& P, cudaStream_t st) { k_tick<<<1, 1, 0, st>>>(P.tstep); }
 
 void launch_jumps(const Dev& P, double E, cudaStream_t st) {
   k_jumps<<<(P.ncross + TPB - 1) / TPB, TPB, 0, st>>>(P, E);

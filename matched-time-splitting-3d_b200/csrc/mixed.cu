@@ -29,6 +29,7 @@ namespace {
 template <int G>
 __global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
                                                    float* __restrict__ rho, double E) {
+  E = step_e(P, E, 2);
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
   const int nrows = P.ny * P.nz;
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ D
                                                        float* __restrict__ rho, double E) {
   const int k = blockIdx.x * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
+  E = step_e(P, E, 2);
   const long long m = P.mibnode[k];
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
@@ -401,7 +403,8 @@ template <int D>
 void sweep32(const Dev& P, float* f, cudaStream_t st) {
   if (P.nblk[D] > 0) k_block_rhs32<D><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
   const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
-  k_sweep32<D, S32_CH, S32_NS, S32_NT><<<P.sweep_blocks, S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f);
+  k_sweep32<D, S32_CH, S32_NS, S32_NT>
+      <<<sweep_grid(P, nlines<D>(P), S32_NT), S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f);
 }
 
 // u^{n+1} = u^n + d, four nodes per thread

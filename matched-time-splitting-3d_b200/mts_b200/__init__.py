@@ -18,7 +18,7 @@ import numpy as np
 from ._lib import (CROSSING_DTYPE, EXPORTS, METHODS, MtsError, check, lib_path, load, make_grid, make_params,
                    make_surface)
 
-__all__ = ["Spec", "Solver", "setup_host", "MtsError", "CROSSING_DTYPE", "METHODS", "EXPORTS", "load", "lib_path"]
+__all__ = ["Spec", "Solver", "setup_host", "batch_advance", "MtsError", "CROSSING_DTYPE", "METHODS", "EXPORTS", "load", "lib_path"]
 
 
 @dataclass
@@ -61,6 +61,18 @@ def setup_host(spec: Spec):
                            cr.ctypes.data if cr.size else None, cr.size, ctypes.byref(count), counts.ctypes.data),
           "mts_setup_host")
     return tags, cr, {"corner_pairs": int(counts[0]), "singular_warnings": int(counts[1])}
+
+
+def batch_advance(solvers, nsteps: int) -> None:
+    """nsteps steps of every solver in one batch (mts_batch_advance): one CUDA
+    graph holding a step of each problem, replayed.  Results equal those of
+    advancing each solver on its own."""
+    solvers = list(solvers)
+    if not solvers:
+        return
+    L = load()
+    arr = (ctypes.c_void_p * len(solvers))(*[s.handle.value for s in solvers])
+    check(L.mts_batch_advance(arr, len(solvers), int(nsteps)), "mts_batch_advance")
 
 
 class Solver:

@@ -39,6 +39,7 @@ EXPORTS = [
     "mts_solve_2nd",
     "mts_advance",
     "mts_advance_host",
+    "mts_batch_advance",
     "mts_norms",
     "mts_norms_noalloc",
     "mts_get_time",
@@ -158,6 +159,7 @@ def load(build_if_missing: bool = True):
             "mts_solve_2nd": [H, ctypes.c_double, ctypes.c_double, ctypes.c_double],
             "mts_advance": [H, ctypes.c_int32],
             "mts_advance_host": [H, vp, vp, ctypes.c_int32],
+            "mts_batch_advance": [vp, ctypes.c_int32, ctypes.c_int32],
             "mts_norms": [H, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_norms_noalloc": [H, vp, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_get_time": [H, P(ctypes.c_double)],
