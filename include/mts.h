@@ -190,6 +190,10 @@ mts_status mts_export_crossings(mts_handle h, mts_crossing* out, int32_t capacit
 /* Number of kernel launches the library has queued on this handle. */
 mts_status mts_get_launch_count(mts_handle h, int64_t* launches);
 
+/* Device memory the handle holds (the sum of its allocations), for callers
+ * that admit problems against a memory budget.  No reference counterpart. */
+mts_status mts_get_device_bytes(mts_handle h, int64_t* bytes);
+
 /* The CUDA stream of the handle (a cudaStream_t), for callers that order
  * their own work against it. */
 mts_status mts_get_stream(mts_handle h, void** stream);

@@ -61,6 +61,7 @@ struct mts_problem {
   double* u0 = nullptr;
   double* u1 = nullptr;
   std::vector<void*> allocations;
+  int64_t device_bytes = 0;  // sum of the allocations' sizes
   double* norm_part = nullptr;
   double* norm_out = nullptr;
   double* host_norm = nullptr;  // pinned, 3 doubles
@@ -88,7 +89,10 @@ struct mts_problem {
   template <class T>
   cudaError_t put(T** dst, const T* src, size_t n) {
     cudaError_t e = upload(dst, src, n, stream);
-    if (*dst) allocations.push_back((void*)*dst);
+    if (*dst) {
+      allocations.push_back((void*)*dst);
+      device_bytes += (n ? n : 1) * sizeof(T);
+    }
     return e;
   }
   // n elements (uploaded from src when given) followed by `pad` zeroed
@@ -96,7 +100,10 @@ struct mts_problem {
   template <class T>
   cudaError_t put_padded(T** dst, const T* src, size_t n, size_t pad) {
     cudaError_t e = upload(dst, (const T*)nullptr, n + pad, stream);
-    if (*dst) allocations.push_back((void*)*dst);
+    if (*dst) {
+      allocations.push_back((void*)*dst);
+      device_bytes += (n + pad) * sizeof(T);
+    }
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(*dst + (src ? n : 0), 0, (src ? pad : n + pad) * sizeof(T), stream);
     if (e != cudaSuccess || !src) return e;
@@ -1022,6 +1029,12 @@ mts_status mts_export_crossings(mts_handle h, mts_crossing* out, int32_t capacit
 mts_status mts_get_launch_count(mts_handle h, int64_t* launches) {
   if (!h || !launches) return fail(MTS_ERR_ARG, "null argument");
   *launches = h->launches;
+  return MTS_OK;
+}
+
+mts_status mts_get_device_bytes(mts_handle h, int64_t* bytes) {
+  if (!h || !bytes) return fail(MTS_ERR_ARG, "null argument");
+  *bytes = h->device_bytes;
   return MTS_OK;
 }
 

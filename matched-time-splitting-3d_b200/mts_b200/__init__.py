@@ -208,6 +208,12 @@ class Solver:
         check(self._L.mts_get_launch_count(self._h, ctypes.byref(v)), "mts_get_launch_count")
         return int(v.value)
 
+    def device_bytes(self) -> int:
+        """Device memory this solver holds (mts_get_device_bytes)."""
+        v = ctypes.c_int64()
+        check(self._L.mts_get_device_bytes(self._h, ctypes.byref(v)), "mts_get_device_bytes")
+        return int(v.value)
+
     def set_profiling(self, on: bool) -> None:
         check(self._L.mts_set_profiling(self._h, 1 if on else 0), "mts_set_profiling")
 

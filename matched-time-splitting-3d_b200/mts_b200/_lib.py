@@ -49,6 +49,7 @@ EXPORTS = [
     "mts_export_tags",
     "mts_export_crossings",
     "mts_get_launch_count",
+    "mts_get_device_bytes",
     "mts_get_stream",
     "mts_set_profiling",
     "mts_profile_read",
@@ -169,6 +170,7 @@ def load(build_if_missing: bool = True):
             "mts_export_tags": [H, vp],
             "mts_export_crossings": [H, vp, ctypes.c_int32, P(ctypes.c_int32)],
             "mts_get_launch_count": [H, P(ctypes.c_int64)],
+            "mts_get_device_bytes": [H, P(ctypes.c_int64)],
             "mts_get_stream": [H, P(ctypes.c_void_p)],
             "mts_set_profiling": [H, ctypes.c_int32],
             "mts_profile_read": [H, vp, vp],
