@@ -80,7 +80,113 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default sweep shapes")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run (ADI only)")
     ap.add_argument("--shapes", default="", help="sweep shapes of the three sweeps, e.g. 4,4,4 (no autotune)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form run")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-form run")
+    ap.add_argument("--batch-problems", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=50)
+    ap.add_argument("--served-requests", type=int, default=1000,
+                    help="requests per arrival rate (the full served workload is 10000)")
+    ap.add_argument("--served-rates", default="200,1000", help="Poisson arrival rates, requests/s")
     return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Batched and served forms (wall-clock: the unit is whole solves, setup of the
+# device state and host work included; the GPU is synchronized at both ends).
+
+def run_batched(count: int, steps: int, seed: int = 0) -> dict:
+    """`count` independent problems of the batched family, `steps` steps each:
+    one problem after another (plain FP64, mts_advance per problem) against
+    all of them in one batch (mts_batch_advance).  Results must agree bit for
+    bit; the solves/s ratio is the batching speed-up."""
+    import torch
+
+    import mts_b200 as M
+    from mts_b200.workloads import batched_problems
+
+    t_setup = time.perf_counter()
+    specs = batched_problems(count, seed)
+    solvers = [M.Solver(sp) for sp in specs]
+    t_setup = time.perf_counter() - t_setup
+    nodes = sum(sp.n[0] * sp.n[1] * sp.n[2] for sp in specs)
+    for s in solvers:
+        s.initialize()
+    torch.cuda.synchronize()
+    # sequential: one problem at a time, each to completion
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.advance(steps)
+        s.synchronize()
+    seq = time.perf_counter() - t0
+    ref = [s.norms() for s in solvers]
+    for s in solvers:
+        s.time = 0.0
+        s.initialize()
+    torch.cuda.synchronize()
+    # batched: every problem in one graph per step pair
+    M.batch_advance(solvers, 1)  # warm: module loading, first graph
+    for s in solvers:
+        s.time = 0.0
+        s.initialize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    M.batch_advance(solvers, steps)
+    bat = time.perf_counter() - t0
+    same = all(s.norms() == r for s, r in zip(solvers, ref))
+    for s in solvers:
+        s.close()
+    return {
+        "problems": count, "steps": steps, "seed": seed, "nodes_total": nodes,
+        "sequential_solves_per_s": count / seq, "batched_solves_per_s": count / bat,
+        "speedup": seq / bat, "batched_cell_steps_per_s": nodes * steps / bat,
+        "sequential_s": seq, "batched_s": bat, "host_setup_s": t_setup, "results_identical": same,
+        "timing": "wall clock between synchronizations (launch and graph overheads included)",
+        "family": "grids U{17,25,33,49,65}^3, shifted ellipsoids, beta_out log-uniform [1e-3,1e3], "
+                  "methods U{ADI,LOD-IE,LOD-CN,TS} x MIB-L1/L2, dt = min h, plain FP64, numpy PCG64 seed 0",
+    }
+
+
+def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 120e9) -> dict:
+    """Poisson streams of `count` requests per rate through the continuous-
+    batching server, against the sequential plain solver on the same stream
+    (its service times measured on a sample, its queue modelled FIFO)."""
+    import numpy as np
+
+    from mts_b200 import serve
+    from mts_b200.workloads import served_requests
+
+    out = {"requests_per_rate": count, "hbm_budget_bytes": budget, "rates": {}}
+    # sequential service time per request (setup, upload, steps, norms), on a
+    # sample of the stream, one request after another
+    sample = served_requests(min(count, 120), 1000.0, seed + 1)
+    svc = []
+    for q in sample:
+        t0 = time.perf_counter()
+        serve.solve_alone(q)
+        svc.append(time.perf_counter() - t0)
+    svc = np.array(svc)
+    out["sequential_solves_per_s"] = float(1.0 / svc.mean())
+    out["sequential_service_sample"] = len(svc)
+    rng = np.random.default_rng(seed + 2)
+    for rate in rates:
+        reqs = served_requests(count, rate, seed)
+        srv = serve.Server(hbm_budget=budget)
+        t0 = time.perf_counter()
+        res = srv.run(reqs)
+        span = time.perf_counter() - t0
+        lat = np.array([r.latency for r in res])
+        arr = np.array([q.arrival for q in reqs])
+        seq_lat = serve.fifo_latencies(arr, rng.choice(svc, len(arr)))
+        out["rates"][str(rate)] = {
+            "solves_per_s": len(res) / span, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "sequential_p50_s": float(np.percentile(seq_lat, 50)),
+            "sequential_p99_s": float(np.percentile(seq_lat, 99)), "peak_active": srv.peak_active,
+            "peak_budget_bytes": srv.peak_bytes, "batches": srv.batches,
+            "solves_per_s_vs_sequential": len(res) / span / out["sequential_solves_per_s"],
+        }
+    out["timing"] = ("wall clock from the first arrival to the last completion; latency = completion - arrival; "
+                     "the sequential latencies model one FIFO solver with the sampled service times")
+    return out
 
 
 def workload(a):
@@ -438,6 +544,10 @@ def main():
     }
     if mixed is not None:
         line["mixed"] = mixed
+    if rank == 0 and world == 1 and not a.no_batched:
+        line["batched"] = run_batched(a.batch_problems, a.batch_steps)
+    if rank == 0 and world == 1 and not a.no_served:
+        line["served"] = run_served(a.served_requests, [float(v) for v in a.served_rates.split(",") if v])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             res = run_reference_sample(w, a.ref_procs or auto_procs(w), 1)

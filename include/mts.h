@@ -126,14 +126,14 @@ mts_status mts_solve_2nd(mts_handle h, double t_prev, double t_half, double t_ne
  * step; TS evaluates at t-dt, t-dt/2, t).  Asynchronous. */
 mts_status mts_advance(mts_handle h, int32_t nsteps);
 
-/* nsteps steps of each of n independent handles, run as one batch: one step
- * of every handle is captured into a single CUDA graph, whose branches the
- * device runs concurrently, and the graph is replayed nsteps times (two
- * steps per graph when a plain Douglas-ADI handle is in the batch).  Each
- * handle's result and time are those of mts_advance(h, nsteps), bit for bit.
- * Handles must be distinct, on one device, with profiling off.  Synchronous.
- * Batches several problems as the reference, which steps one problem per
- * process (helper.h:199-426), has no counterpart for. */
+/* nsteps steps of each of n independent handles, run as one batch: the
+ * plain-form handles of one method advance together, one kernel launch per
+ * kernel of the step for all of them (each CTA carries its problem and its
+ * place in that problem's grid); mixed-precision handles step on their own
+ * streams alongside.  Each handle's result and time are those of
+ * mts_advance(h, nsteps), bit for bit.  Handles must be distinct, on one
+ * device, with profiling off.  Synchronous.  No counterpart in the
+ * reference, which steps one problem per process (helper.h:199-426). */
 mts_status mts_batch_advance(const mts_handle* handles, int32_t n, int32_t nsteps);
 
 /* The same loop with the caller's host field: u_in is uploaded, nsteps steps

@@ -447,6 +447,7 @@ mts_status finish_create(mts_problem* h) {
   if (!configured) {
     mts::configure_kernels();
     mts::configure_mixed_kernels();
+    mts::configure_batch_kernels();
     configured = true;
   }
   int sms = 0;
@@ -476,6 +477,8 @@ mts_status finish_create(mts_problem* h) {
   const size_t fpad = (size_t)mts::kRowPad * (size_t)g.nx * (size_t)g.ny;
   CUDA_TRY(h->put_padded(&h->u0, (const double*)nullptr, (size_t)N, fpad));
   CUDA_TRY(h->put_padded(&h->u1, (const double*)nullptr, (size_t)N, fpad));
+  D.u0 = h->u0;
+  D.u1 = h->u1;
   CUDA_TRY(h->put_padded(&D.dp, (const double*)nullptr, (size_t)nmax * tmax, (size_t)mts::kRowPad * tmax));
   for (int d = 0; d < 3; d++) {
     for (int side = 0; side < 2; side++) {
@@ -763,15 +766,14 @@ mts_status mts_advance(mts_handle h, int32_t nsteps) {
   return advance(h, nsteps);
 }
 
-// Batched stepping.  Each handle keeps its own device state and kernels; one
-// step of every handle is captured into a single CUDA graph (the handles'
-// launches are independent branches that the device runs concurrently) and
-// the graph is replayed.  A replay must not bake in the step's times, so each
-// handle gets a table of its per-step exp(-t) factors, computed here exactly as
-// advance() computes them, and a device step counter that the graph advances;
-// the kernels read the factors from the table.  Plain Douglas-ADI swaps its
-// two fields every step, so graphs hold two steps when such a handle is in
-// the batch.
+// Batched stepping.  Handles of the plain form are grouped by method; a
+// group advances with one launch per kernel of the step for all its problems
+// (mts::launch_step_batch: each CTA of a launch carries its problem and its
+// place in that problem's own grid, so every problem computes exactly what
+// its own launches would).  Mixed-precision handles step on their own
+// streams.  Every handle reads its step's exp(-t) factors from a table
+// computed here exactly as advance() computes them, indexed by a device step
+// counter that each step advances, so batching changes no bit of any result.
 mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
   if (!hs || n < 1 || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
   for (int i = 0; i < n; i++) {
@@ -782,29 +784,16 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
     if (hs[i]->profiling) return fail(MTS_ERR_ARG, "profiling is on for a batch handle");
   }
   if (nsteps == 0) return MTS_OK;
-  struct Sched {
-    double* tab = nullptr;
-    int* step = nullptr;
-    double t_end = 0;
-    int64_t graph_launches = 0;
-  };
-  std::vector<Sched> sc((size_t)n);
-  cudaStream_t root = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  std::vector<cudaEvent_t> evs;
+  std::vector<void*> dev_alloc;  // freed at the end
+  std::vector<cudaStream_t> streams;
+  std::vector<double> t_end((size_t)n);
   mts_status st = MTS_OK;
   auto cleanup = [&]() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    for (cudaEvent_t e : evs)
-      if (e) cudaEventDestroy(e);
-    if (root) cudaStreamDestroy(root);
+    for (cudaStream_t q : streams) cudaStreamDestroy(q);
+    for (void* q : dev_alloc) cudaFree(q);
     for (int i = 0; i < n; i++) {
       hs[i]->dev.tsched = nullptr;
       hs[i]->dev.tstep = nullptr;
-      if (sc[(size_t)i].tab) cudaFree(sc[(size_t)i].tab);
-      if (sc[(size_t)i].step) cudaFree(sc[(size_t)i].step);
     }
   };
 #define BATCH_TRY(call)                                                                          \
@@ -817,10 +806,16 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
       return st;                                                                                 \
     }                                                                                            \
   } while (0)
-  bool two = false;
+  auto dev_upload = [&](const void* src, size_t bytes, cudaStream_t q, void** out) -> cudaError_t {
+    *out = nullptr;
+    cudaError_t e = cudaMalloc(out, bytes ? bytes : 16);
+    if (e != cudaSuccess) return e;
+    dev_alloc.push_back(*out);
+    return bytes ? cudaMemcpyAsync(*out, src, bytes, cudaMemcpyHostToDevice, q) : cudaSuccess;
+  };
+  // step tables and counters
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
-    if (h->prm.method == MTS_ADI && h->dev.precision == 0) two = true;
     std::vector<double> tab(3 * (size_t)nsteps);
     double t = h->t;
     const double dt = h->prm.dt;
@@ -831,63 +826,87 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
       tab[3 * (size_t)k + 2] = std::exp(-t1);
       t = t1;
     }
-    sc[(size_t)i].t_end = t;
-    BATCH_TRY(cudaMalloc((void**)&sc[(size_t)i].tab, tab.size() * sizeof(double)));
-    BATCH_TRY(cudaMalloc((void**)&sc[(size_t)i].step, sizeof(int)));
-    BATCH_TRY(cudaMemcpyAsync(sc[(size_t)i].tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice,
-                              h->stream));
-    BATCH_TRY(cudaMemsetAsync(sc[(size_t)i].step, 0, sizeof(int), h->stream));
-    BATCH_TRY(cudaStreamSynchronize(h->stream));
-    h->dev.tsched = sc[(size_t)i].tab;
-    h->dev.tstep = sc[(size_t)i].step;
+    t_end[(size_t)i] = t;
+    const int zero = 0;
+    void *tab_d = nullptr, *step_d = nullptr;
+    BATCH_TRY(dev_upload(tab.data(), tab.size() * sizeof(double), h->stream, &tab_d));
+    BATCH_TRY(dev_upload(&zero, sizeof(int), h->stream, &step_d));
+    BATCH_TRY(cudaStreamSynchronize(h->stream));  // also: the handle's earlier work is done
+    h->dev.tsched = (const double*)tab_d;
+    h->dev.tstep = (int*)step_d;
   }
-  const int g = two ? 2 : 1;
-  auto enqueue = [&](mts_problem* h, int steps) {
-    int64_t c = 0;
-    for (int k = 0; k < steps; k++) {
-      mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
-      if (h->dev.precision == 1)
-        c += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr);
-      else
-        c += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, nullptr);
-      mts::launch_tick(h->dev, h->stream);
-      c++;
+  // plain handles by method: one batched launch sequence per group
+  for (int method = 0; method < 4; method++) {
+    std::vector<int> mem;
+    for (int i = 0; i < n; i++)
+      if (hs[i]->dev.precision == 0 && hs[i]->prm.method == method) mem.push_back(i);
+    if (mem.empty()) continue;
+    cudaStream_t q = nullptr;
+    BATCH_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+    streams.push_back(q);
+    std::vector<mts::Dev> recs;
+    mts::BatchPlan plan{};
+    plan.method = method;
+    plan.n = (int)mem.size();
+    std::vector<mts::BatchItem> jumps, rows, mib, blk[3], sw[3];
+    auto add = [](std::vector<mts::BatchItem>& v, int p, unsigned ncta) {
+      for (unsigned c = 0; c < ncta; c++) v.push_back(mts::BatchItem{p, (int32_t)c, (int32_t)ncta, 0});
+    };
+    for (int k = 0; k < (int)mem.size(); k++) {
+      const mts::Dev& d = hs[mem[(size_t)k]]->dev;
+      recs.push_back(d);
+      plan.nmax = std::max(plan.nmax, std::max(d.nx, std::max(d.ny, d.nz)));
+      if (d.ncross > 0) add(jumps, k, mts::jumps_grid(d));
+      add(rows, k, mts::pointwise_rows_grid(d));
+      if (d.nmibnode > 0) add(mib, k, mts::mib_grid(d));
+      for (int dd = 0; dd < 3; dd++) {
+        if (d.nblk[dd] > 0) add(blk[dd], k, mts::block_grid(d, dd));
+        add(sw[dd], k, mts::batch_sweep_grid(d, dd));
+      }
     }
-    return c;
-  };
-  const int replays = nsteps / g;
-  BATCH_TRY(cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking));
-  evs.assign((size_t)n + 2, nullptr);
-  for (auto& e : evs) BATCH_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  if (replays > 0) {
-    BATCH_TRY(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal));
-    BATCH_TRY(cudaEventRecord(evs[(size_t)n], root));
-    for (int i = 0; i < n; i++) {
-      mts_problem* h = hs[i];
-      BATCH_TRY(cudaStreamWaitEvent(h->stream, evs[(size_t)n], 0));
-      sc[(size_t)i].graph_launches = enqueue(h, g);
-      BATCH_TRY(cudaEventRecord(evs[(size_t)i], h->stream));
-      BATCH_TRY(cudaStreamWaitEvent(root, evs[(size_t)i], 0));
+    void* tmp = nullptr;
+    BATCH_TRY(dev_upload(recs.data(), recs.size() * sizeof(mts::Dev), q, &tmp));
+    plan.Ps = (const mts::Dev*)tmp;
+    auto up = [&](std::vector<mts::BatchItem>& v, const mts::BatchItem** dst, int* cnt) -> cudaError_t {
+      *cnt = (int)v.size();
+      void* p = nullptr;
+      cudaError_t e = dev_upload(v.data(), v.size() * sizeof(mts::BatchItem), q, &p);
+      *dst = (const mts::BatchItem*)p;
+      return e;
+    };
+    BATCH_TRY(up(jumps, &plan.jumps, &plan.njumps));
+    BATCH_TRY(up(rows, &plan.rows, &plan.nrows));
+    BATCH_TRY(up(mib, &plan.mib, &plan.nmib));
+    for (int dd = 0; dd < 3; dd++) {
+      BATCH_TRY(up(blk[dd], &plan.blk[dd], &plan.nblk[dd]));
+      BATCH_TRY(up(sw[dd], &plan.sw[dd], &plan.nsw[dd]));
     }
-    BATCH_TRY(cudaStreamEndCapture(root, &graph));
-    BATCH_TRY(cudaGraphInstantiate(&exec, graph, 0));
-    for (int r = 0; r < replays; r++) BATCH_TRY(cudaGraphLaunch(exec, root));
-    for (int i = 0; i < n; i++) hs[i]->launches += sc[(size_t)i].graph_launches * replays;
+    // the host vectors must outlive the asynchronous uploads
+    BATCH_TRY(cudaStreamSynchronize(q));
+    int64_t launches = 0;
+    for (int k = 0; k < nsteps; k++) launches += mts::launch_step_batch(plan, q);
+    BATCH_TRY(cudaGetLastError());
+    for (int i : mem) hs[i]->launches += launches;
+    BATCH_TRY(cudaStreamSynchronize(q));
   }
-  // a step left over (odd count with two-step graphs) runs outside the graph
-  BATCH_TRY(cudaEventRecord(evs[(size_t)n + 1], root));
+  // mixed-precision handles: their own steps on their own streams
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
-    BATCH_TRY(cudaStreamWaitEvent(h->stream, evs[(size_t)n + 1], 0));
-    h->launches += enqueue(h, nsteps - replays * g);
+    if (h->dev.precision != 1) continue;
+    for (int k = 0; k < nsteps; k++) {
+      mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
+      h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr);
+      mts::launch_tick(h->dev, h->stream);
+      h->launches++;
+    }
+    BATCH_TRY(cudaGetLastError());
   }
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
     mts_status s2 = sync_status(h);
     if (s2 && !st) st = s2;
-    h->t = sc[(size_t)i].t_end;
+    h->t = t_end[(size_t)i];
   }
-  BATCH_TRY(cudaStreamSynchronize(root));
   cleanup();
 #undef BATCH_TRY
   return st;

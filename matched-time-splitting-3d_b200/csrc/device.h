@@ -114,6 +114,8 @@ struct Dev {
   // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
   const double* tsched;
   int* tstep;
+  double* u0;  // the state (every method keeps it here)
+  double* u1;  // scratch field
   const long long* mibnode;  // nodes with a MIB flag (any direction), ascending
   int nmibnode;
   int* status;       // reserved
@@ -142,6 +144,38 @@ int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t 
 void configure_mixed_kernels();
 int mixed_sweep_threads();            // threads per CTA of the FP32 sweeps
 bool mixed_shape_fits(int nmax);      // their shared memory within the limit
+// Batched plain steps (kernels.cu): problems of one method advance together,
+// one launch per kernel of the step for all of them.  A launch's CTAs are
+// listed as items (problem, the CTA's index in that problem's own grid, the
+// size of that grid), so every problem sees exactly the grid its own launch
+// would have; the problems' Dev records live in device memory.
+struct BatchItem {
+  int32_t p, cta, ncta, pad;
+};
+struct BatchPlan {
+  int method;         // MTS_ADI .. MTS_TS, shared by all problems
+  int n;              // problems
+  int nmax;           // longest line over the problems
+  const Dev* Ps;      // [n] device records (tsched/tstep set)
+  const BatchItem* jumps;
+  int njumps;
+  const BatchItem* rows;  // pointwise passes over grid rows
+  int nrows;
+  const BatchItem* mib;   // MIB node list passes
+  int nmib;
+  const BatchItem* blk[3];  // block pre-pass per direction
+  int nblk[3];
+  const BatchItem* sw[3];   // line sweeps per direction
+  int nsw[3];
+};
+int batch_sweep_threads();                 // threads per CTA of the batched sweeps
+void configure_batch_kernels();
+int launch_step_batch(const BatchPlan& plan, cudaStream_t stream);  // one step + tick
+unsigned jumps_grid(const Dev& P);
+unsigned mib_grid(const Dev& P);
+unsigned block_grid(const Dev& P, int d);
+unsigned batch_sweep_grid(const Dev& P, int d);
+
 // Shared by both step forms (kernels.cu).
 void launch_jumps(const Dev& P, double E, cudaStream_t stream);
 void launch_tick(const Dev& P, cudaStream_t stream);  // ++(*P.tstep)

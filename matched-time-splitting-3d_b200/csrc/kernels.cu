@@ -97,8 +97,7 @@ __device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __rest
 }
 
 template <int G>
-__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                 double* __restrict__ R, double E) {
+__device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ un, double* __restrict__ R, double E) {
   E = step_e(P, E, 2);
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
@@ -109,7 +108,7 @@ __global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, 
   const double y0o = P.vd[1][1][0], y1o = P.vd[1][1][1], y2o = P.vd[1][1][2];
   const double z0i = P.vd[2][0][0], z1i = P.vd[2][0][1], z2i = P.vd[2][0][2];
   const double z0o = P.vd[2][1][0], z1o = P.vd[2][1][1], z2o = P.vd[2][1][2];
-  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+  for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)P.nx * row;
     const RowExact q = row_exact(P, iy, iz);
@@ -166,16 +165,24 @@ __global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, 
   }
 }
 
+template <int G>
+__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un, double* __restrict__ R, double E) {
+  k_adi_rhs_body<G>(P, blockIdx.x, gridDim.x, un, R, E);
+}
+
 // The MIB rows of RHS1, one thread per listed node.
-__global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                     double* __restrict__ R, double E) {
-  const int k = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void k_adi_rhs_mib_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ un, double* __restrict__ R, double E) {
+  const int k = cta_ * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   E = step_e(P, E, 2);
   const long long m = P.mibnode[k];
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
   R[m] = adi_rhs_mib(P, un, E, m, ix, iy, iz, P.tag[m]);
+}
+
+__global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev P, const double* __restrict__ un, double* __restrict__ R, double E) {
+  k_adi_rhs_mib_body(P, blockIdx.x, gridDim.x, un, R, E);
 }
 
 // TS explicit half step along D = x or y (TS::D_xx_r / D_yy_r, the LOD
@@ -201,9 +208,8 @@ __device__ __forceinline__ double ts_explicit_mib(const Dev& P, const double* __
 }
 
 template <int D>
-__global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__ Dev P, const double* __restrict__ in,
-                                                         double* __restrict__ out) {
-  const int k = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void k_ts_explicit_mib_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ in, double* __restrict__ out) {
+  const int k = cta_ * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   const long long m = P.mibnode[k];
   const int tg = P.tag[m];
@@ -214,8 +220,12 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__
 }
 
 template <int D>
-__global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in,
-                                                     double* __restrict__ out, double eh) {
+__global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__ Dev P, const double* __restrict__ in, double* __restrict__ out) {
+  k_ts_explicit_mib_body<D>(P, blockIdx.x, gridDim.x, in, out);
+}
+
+template <int D>
+__device__ __forceinline__ void k_ts_explicit_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ in, double* __restrict__ out, double eh) {
   eh = step_e(P, eh, 1);
   const long long s = D == 0 ? 1 : (long long)P.nx;
   const int flag = D == 0 ? TAG_MIBX : TAG_MIBY;
@@ -224,7 +234,7 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev
   const double kex = P.kex;
   const double w0i = P.vd[D][0][0], w1i = P.vd[D][0][1], w2i = P.vd[D][0][2];
   const double w0o = P.vd[D][1][0], w1o = P.vd[D][1][1], w2o = P.vd[D][1][2];
-  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+  for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)P.nx * row;
     const RowExact q = row_exact(P, iy, iz);
@@ -268,6 +278,11 @@ __global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev
       }
     }
   }
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in, double* __restrict__ out, double eh) {
+  k_ts_explicit_body<D>(P, blockIdx.x, gridDim.x, in, out, eh);
 }
 
 // ---------------------------------------------------------------------------
@@ -318,8 +333,8 @@ __device__ __forceinline__ void load_head(const MibBlock* blk, const double* rbl
 // terms of D_xx_l lod.cc:960-1097, the Convert2Tri row operations) and stores
 // them for the sweep, which then spends no time on MIB data.
 template <int D, int KIND>
-__global__ void __launch_bounds__(TPB) k_block_rhs(const Dev P, const SweepIO io, int nblk) {
-  const int k = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void k_block_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_, const SweepIO io, int nblk) {
+  const int k = cta_ * TPB + threadIdx.x;
   if (k >= nblk) return;
   const MibBlock& b = P.blk[D][k];
   const int n2 = D == 2 ? P.ny : P.nz;
@@ -350,6 +365,11 @@ __global__ void __launch_bounds__(TPB) k_block_rhs(const Dev P, const SweepIO io
   implicit_rows(P, b, r, P.vd[D][b.sides & 1], P.vd[D][(b.sides >> 1) & 1], P.vd[D][(b.sides >> 2) & 1], io.jumps,
                 P.jv);
   for (int q = 0; q < 3; q++) P.rblk[D][3 * k + q] = r[q];
+}
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(TPB) k_block_rhs(const __grid_constant__ Dev P, const SweepIO io, int nblk) {
+  k_block_rhs_body<D, KIND>(P, blockIdx.x, gridDim.x, io, nblk);
 }
 
 // Exact-solution parts along a line: the fixed axes are read once per line,
@@ -409,7 +429,7 @@ constexpr size_t shape_smem(int n) {
 
 
 template <int D, int KIND, int CH, int NS, int NT>
-__global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) {
+__device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsigned ncta_, const SweepIO io) {
   static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4, "shape");
   static_assert(CH <= kRowPad, "chunk rows past a line end must stay within the fields' slack");
   constexpr int RING = NS * CH;    // rows in a field's ring
@@ -422,8 +442,8 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
 #define SA(j) sA[((j) & (RING - 1)) * NT]
 #define SB(j) sB[((j) & (RING - 1)) * NT]
 #define SC(j) sC[((j) & (RING - 1)) * NT]
-  const long long T = (long long)gridDim.x * NT;
-  const long long gt = (long long)blockIdx.x * NT + tid;
+  const long long T = (long long)ncta_ * NT;
+  const long long gt = (long long)cta_ * NT + tid;
   double* const dp = P.dp + gt;
   const long long nl = nlines<D>(P);
   const MibBlock* __restrict__ blk = P.blk[D];
@@ -722,9 +742,14 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const Dev P, const SweepIO io) 
 #undef SC
 }
 
+template <int D, int KIND, int CH, int NS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_sweep(const __grid_constant__ Dev P, const SweepIO io) {
+  k_sweep_body<D, KIND, CH, NS, NT>(P, blockIdx.x, gridDim.x, io);
+}
+
 // Refresh_Jump (intersection.cc:2294-2490): [u] and u_dir per crossing.
-__global__ void __launch_bounds__(TPB) k_jumps(const Dev P, double E) {
-  int c = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void k_jumps_body(const Dev& P, unsigned cta_, unsigned ncta_, double E) {
+  int c = cta_ * TPB + threadIdx.x;
   if (c >= P.ncross) return;
   E = step_e(P, E, 2);
   const CrossConst q = P.cc[c];
@@ -739,6 +764,10 @@ __global__ void __launch_bounds__(TPB) k_jumps(const Dev P, double E) {
   }
   double bxi = q.p[0] * jb[0] + q.p[1] * jb[1] + q.p[2] * jb[2];
   P.jv[c] = make_double2(ju, q.pinv * bxi);
+}
+
+__global__ void __launch_bounds__(TPB) k_jumps(const __grid_constant__ Dev P, double E) {
+  k_jumps_body(P, blockIdx.x, gridDim.x, E);
 }
 
 __global__ void __launch_bounds__(TPB) k_init(const Dev P, double E, double* u) {
@@ -935,7 +964,9 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
   if (P.method == 0) {
     // Douglas-ADI.  u1 <- uhs (pointwise); x sweep in place gives u*; y sweep
     // builds uhss = -dt D_yy u^n + u* and solves in place (u**); z sweep builds
-    // uh1 = -dt D_zz u^n + u** and solves in place (u^{n+1}).
+    // uh1 = -dt D_zz u^n + u** and writes u^{n+1} over u^n in u0 (a z line
+    // reads only its own nodes of u^n; its faces get Outer_u(t_next), the
+    // value u** holds there).  The state stays in u0, u1 is scratch.
     mark(0);
     k_adi_rhs<2><<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_next);
     if (P.nmibnode > 0) {
@@ -956,13 +987,12 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
     mark(0);
     sweep<1, K_STENCIL>(P, io, P.shape[1], st);
     mark(1);
+    io.out = u0;
+    io.bmode = 1;
     mark(0);
     sweep<2, K_STENCIL>(P, io, P.shape[2], st);
     mark(1);
     launches += 4;
-    double* tmp = u0;
-    u0 = u1;
-    u1 = tmp;
   } else if (P.method == 1 || P.method == 2) {
     // LOD, in place on u0.
     io.jumps = 1;
@@ -1128,6 +1158,181 @@ __global__ void __launch_bounds__(NB_TPB) k_norms_noalloc(const Dev P, double E,
 int launch_norms_noalloc(const Dev& P, double E, const double* u, double* scratch, int nb, cudaStream_t st) {
   k_norms_noalloc<<<nb, NB_TPB, 0, st>>>(P, E, u, scratch);
   return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Batched plain steps: the kernels above, launched once for many problems.
+
+namespace {
+
+struct Roles {
+  int stin, add, out;  // fields: 0 = u0, 1 = u1
+  int ksel;            // explicit factor: 0 none, 1 -dt (ADI), 2 0.5*dt (LOD-CN, TS)
+  int jumps, bmode, last;
+};
+
+__device__ __forceinline__ SweepIO make_io(const Dev& P, const Roles& r) {
+  SweepIO io{};
+  io.stin = r.stin ? P.u1 : P.u0;
+  io.add = r.add ? P.u1 : P.u0;
+  io.out = r.out ? P.u1 : P.u0;
+  io.k = r.ksel == 1 ? -P.dt : r.ksel == 2 ? P.kex : 0.0;
+  io.jumps = r.jumps;
+  io.bmode = r.bmode;
+  io.last = r.last;
+  io.e0 = io.e1 = 0.0;  // from the step table
+  return io;
+}
+
+// The CTA's item and its problem's record, copied into shared memory.
+#define BATCH_PROLOGUE                                                                \
+  __shared__ __align__(16) long long sdev_[(sizeof(Dev) + 7) / 8];                    \
+  const BatchItem w = items[blockIdx.x];                                              \
+  {                                                                                   \
+    const long long* src_ = reinterpret_cast<const long long*>(Ps + w.p);             \
+    for (int i_ = threadIdx.x; i_ < (int)((sizeof(Dev) + 7) / 8); i_ += blockDim.x) \
+      sdev_[i_] = src_[i_];                                                           \
+  }                                                                                   \
+  __syncthreads();                                                                    \
+  const Dev& P = *reinterpret_cast<const Dev*>(sdev_);
+
+__global__ void __launch_bounds__(TPB) kb_jumps(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  k_jumps_body(P, w.cta, w.ncta, 0.0);
+}
+
+__global__ void __launch_bounds__(TPB) kb_adi_rhs(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  k_adi_rhs_body<2>(P, w.cta, w.ncta, P.u0, P.u1, 0.0);
+}
+
+__global__ void __launch_bounds__(TPB) kb_adi_rhs_mib(const Dev* __restrict__ Ps,
+                                                      const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  k_adi_rhs_mib_body(P, w.cta, w.ncta, P.u0, P.u1, 0.0);
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) kb_ts_explicit(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items,
+                                                      int in) {
+  BATCH_PROLOGUE
+  k_ts_explicit_body<D>(P, w.cta, w.ncta, in ? P.u1 : P.u0, in ? P.u0 : P.u1, 0.0);
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) kb_ts_explicit_mib(const Dev* __restrict__ Ps,
+                                                          const BatchItem* __restrict__ items, int in) {
+  BATCH_PROLOGUE
+  k_ts_explicit_mib_body<D>(P, w.cta, w.ncta, in ? P.u1 : P.u0, in ? P.u0 : P.u1);
+}
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(TPB) kb_block_rhs(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items,
+                                                    Roles r) {
+  BATCH_PROLOGUE
+  k_block_rhs_body<D, KIND>(P, w.cta, w.ncta, make_io(P, r), P.nblk[D]);
+}
+
+// the small-CTA shape (several CTAs per SM) for batches of small problems
+constexpr int BCH = 4, BNS = 4, BNT = 128;
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(BNT) kb_sweep(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items,
+                                                Roles r) {
+  BATCH_PROLOGUE
+  k_sweep_body<D, KIND, BCH, BNS, BNT>(P, w.cta, w.ncta, make_io(P, r));
+}
+
+__global__ void kb_tick(const Dev* __restrict__ Ps, int n) {
+  const int i = blockIdx.x * TPB + threadIdx.x;
+  if (i < n) ++*Ps[i].tstep;
+}
+
+template <int D, int KIND>
+void bsweep(const BatchPlan& b, const Roles& r, cudaStream_t st, int& launches) {
+  if (b.nblk[D] > 0) {
+    kb_block_rhs<D, KIND><<<b.nblk[D], TPB, 0, st>>>(b.Ps, b.blk[D], r);
+    launches++;
+  }
+  if (b.nsw[D] > 0) {
+    kb_sweep<D, KIND><<<b.nsw[D], BNT, shape_smem<BCH, BNS, BNT>(b.nmax), st>>>(b.Ps, b.sw[D], r);
+    launches++;
+  }
+}
+
+template <int D, int KIND>
+void bsweep_attr() {
+  cudaFuncSetAttribute(kb_sweep<D, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kMaxSweepSmem - (int)sizeof(Dev) - 64);
+}
+
+}  // namespace
+
+int batch_sweep_threads() { return BNT; }
+
+unsigned jumps_grid(const Dev& P) { return (unsigned)((P.ncross + TPB - 1) / TPB); }
+unsigned mib_grid(const Dev& P) { return (unsigned)((P.nmibnode + TPB - 1) / TPB); }
+unsigned block_grid(const Dev& P, int d) { return (unsigned)((P.nblk[d] + TPB - 1) / TPB); }
+unsigned batch_sweep_grid(const Dev& P, int d) {
+  return sweep_grid(P, d == 0 ? nlines<0>(P) : d == 1 ? nlines<1>(P) : nlines<2>(P), BNT);
+}
+
+void configure_batch_kernels() {
+  bsweep_attr<0, K_COPY>();
+  bsweep_attr<1, K_COPY>();
+  bsweep_attr<2, K_COPY>();
+  bsweep_attr<0, K_STENCIL>();
+  bsweep_attr<1, K_STENCIL>();
+  bsweep_attr<2, K_STENCIL>();
+  bsweep_attr<2, K_TS_Z>();
+}
+
+// One step of every problem of the plan, the launch sequence of launch_step.
+int launch_step_batch(const BatchPlan& b, cudaStream_t st) {
+  int launches = 0;
+  if (b.njumps > 0) {
+    kb_jumps<<<b.njumps, TPB, 0, st>>>(b.Ps, b.jumps);
+    launches++;
+  }
+  if (b.method == 0) {
+    kb_adi_rhs<<<b.nrows, TPB, 0, st>>>(b.Ps, b.rows);
+    launches++;
+    if (b.nmib > 0) {
+      kb_adi_rhs_mib<<<b.nmib, TPB, 0, st>>>(b.Ps, b.mib);
+      launches++;
+    }
+    bsweep<0, K_COPY>(b, Roles{1, 1, 1, 0, 0, 0, 0}, st, launches);
+    bsweep<1, K_STENCIL>(b, Roles{0, 1, 1, 1, 0, 0, 0}, st, launches);
+    bsweep<2, K_STENCIL>(b, Roles{0, 1, 0, 1, 0, 1, 0}, st, launches);
+  } else if (b.method == 1 || b.method == 2) {
+    if (b.method == 2) {
+      bsweep<0, K_STENCIL>(b, Roles{0, 0, 0, 2, 1, 1, 0}, st, launches);
+      bsweep<1, K_STENCIL>(b, Roles{0, 0, 0, 2, 1, 1, 0}, st, launches);
+      bsweep<2, K_STENCIL>(b, Roles{0, 0, 0, 2, 1, 2, 1}, st, launches);
+    } else {
+      bsweep<0, K_COPY>(b, Roles{0, 0, 0, 2, 1, 1, 0}, st, launches);
+      bsweep<1, K_COPY>(b, Roles{0, 0, 0, 2, 1, 1, 0}, st, launches);
+      bsweep<2, K_COPY>(b, Roles{0, 0, 0, 2, 1, 2, 1}, st, launches);
+    }
+  } else {
+    kb_ts_explicit<0><<<b.nrows, TPB, 0, st>>>(b.Ps, b.rows, 0);
+    launches++;
+    if (b.nmib > 0) {
+      kb_ts_explicit_mib<0><<<b.nmib, TPB, 0, st>>>(b.Ps, b.mib, 0);
+      launches++;
+    }
+    kb_ts_explicit<1><<<b.nrows, TPB, 0, st>>>(b.Ps, b.rows, 1);
+    launches++;
+    if (b.nmib > 0) {
+      kb_ts_explicit_mib<1><<<b.nmib, TPB, 0, st>>>(b.Ps, b.mib, 1);
+      launches++;
+    }
+    bsweep<2, K_TS_Z>(b, Roles{0, 0, 0, 2, 1, 1, 0}, st, launches);
+    bsweep<1, K_COPY>(b, Roles{0, 0, 0, 2, 1, 0, 0}, st, launches);
+    bsweep<0, K_COPY>(b, Roles{0, 0, 0, 2, 1, 0, 0}, st, launches);
+  }
+  kb_tick<<<(b.n + TPB - 1) / TPB, TPB, 0, st>>>(b.Ps, b.n);
+  return launches + 1;
 }
 
 }  // namespace mts
