@@ -136,6 +136,12 @@ mts_status mts_advance(mts_handle h, int32_t nsteps);
  * reference, which steps one problem per process (helper.h:199-426). */
 mts_status mts_batch_advance(const mts_handle* handles, int32_t n, int32_t nsteps);
 
+/* The same with a step count per handle (counts[i] steps for handles[i]):
+ * the batched launches run for the longest count and skip each problem once
+ * its own steps are done, so problems with different remaining work share
+ * one batch.  Used by the continuous-batching server. */
+mts_status mts_batch_advance_steps(const mts_handle* handles, const int32_t* counts, int32_t n);
+
 /* The same loop with the caller's host field: u_in is uploaded, nsteps steps
  * run, the result is downloaded into u_out (which may equal u_in).  This is
  * the per-call cost of the reference's Solve_2nd(..., CubicDoub& uh, ...)

@@ -776,6 +776,17 @@ mts_status mts_advance(mts_handle h, int32_t nsteps) {
 // counter that each step advances, so batching changes no bit of any result.
 mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
   if (!hs || n < 1 || nsteps < 0) return fail(MTS_ERR_ARG, "bad argument");
+  std::vector<int32_t> counts((size_t)n, nsteps);
+  return mts_batch_advance_steps(hs, counts.data(), n);
+}
+
+mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, int32_t n) {
+  if (!hs || !counts || n < 1) return fail(MTS_ERR_ARG, "bad argument");
+  int32_t nsteps = 0;
+  for (int i = 0; i < n; i++) {
+    if (counts[i] < 0) return fail(MTS_ERR_ARG, "negative step count");
+    nsteps = std::max(nsteps, counts[i]);
+  }
   for (int i = 0; i < n; i++) {
     if (!hs[i]) return fail(MTS_ERR_ARG, "null handle in batch");
     for (int k = 0; k < i; k++)
@@ -813,27 +824,35 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
     dev_alloc.push_back(*out);
     return bytes ? cudaMemcpyAsync(*out, src, bytes, cudaMemcpyHostToDevice, q) : cudaSuccess;
   };
-  // step tables and counters
-  for (int i = 0; i < n; i++) {
-    mts_problem* h = hs[i];
-    std::vector<double> tab(3 * (size_t)nsteps);
-    double t = h->t;
-    const double dt = h->prm.dt;
-    for (int k = 0; k < nsteps; k++) {
-      const double t1 = t + dt;
-      tab[3 * (size_t)k] = std::exp(-(t1 - dt));
-      tab[3 * (size_t)k + 1] = std::exp(-(t1 - 0.5 * dt));
-      tab[3 * (size_t)k + 2] = std::exp(-t1);
-      t = t1;
+  // step tables and counters, one allocation each for the whole batch
+  {
+    std::vector<double> tab(3 * (size_t)nsteps * (size_t)n);
+    for (int i = 0; i < n; i++) {
+      mts_problem* h = hs[i];
+      double t = h->t;
+      const double dt = h->prm.dt;
+      double* row = tab.data() + 3 * (size_t)nsteps * (size_t)i;
+      for (int k = 0; k < counts[i]; k++) {
+        const double t1 = t + dt;
+        row[3 * (size_t)k] = std::exp(-(t1 - dt));
+        row[3 * (size_t)k + 1] = std::exp(-(t1 - 0.5 * dt));
+        row[3 * (size_t)k + 2] = std::exp(-t1);
+        t = t1;
+      }
+      t_end[(size_t)i] = t;
+      BATCH_TRY(cudaStreamSynchronize(h->stream));  // the handle's earlier work is done
     }
-    t_end[(size_t)i] = t;
-    const int zero = 0;
+    std::vector<int> zeros((size_t)n, 0);
     void *tab_d = nullptr, *step_d = nullptr;
-    BATCH_TRY(dev_upload(tab.data(), tab.size() * sizeof(double), h->stream, &tab_d));
-    BATCH_TRY(dev_upload(&zero, sizeof(int), h->stream, &step_d));
-    BATCH_TRY(cudaStreamSynchronize(h->stream));  // also: the handle's earlier work is done
-    h->dev.tsched = (const double*)tab_d;
-    h->dev.tstep = (int*)step_d;
+    cudaStream_t q0 = hs[0]->stream;
+    BATCH_TRY(dev_upload(tab.data(), tab.size() * sizeof(double), q0, &tab_d));
+    BATCH_TRY(dev_upload(zeros.data(), zeros.size() * sizeof(int), q0, &step_d));
+    BATCH_TRY(cudaStreamSynchronize(q0));
+    for (int i = 0; i < n; i++) {
+      hs[i]->dev.tsched = (const double*)tab_d + 3 * (size_t)nsteps * (size_t)i;
+      hs[i]->dev.tstep = (int*)step_d + i;
+      hs[i]->dev.tstop = counts[i];
+    }
   }
   // plain handles by method: one batched launch sequence per group
   for (int method = 0; method < 4; method++) {
@@ -883,8 +902,10 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
     }
     // the host vectors must outlive the asynchronous uploads
     BATCH_TRY(cudaStreamSynchronize(q));
+    int gsteps = 0;  // the group's longest count: later steps skip finished problems
+    for (int i : mem) gsteps = std::max(gsteps, counts[i]);
     int64_t launches = 0;
-    for (int k = 0; k < nsteps; k++) launches += mts::launch_step_batch(plan, q);
+    for (int k = 0; k < gsteps; k++) launches += mts::launch_step_batch(plan, q);
     BATCH_TRY(cudaGetLastError());
     for (int i : mem) hs[i]->launches += launches;
     BATCH_TRY(cudaStreamSynchronize(q));
@@ -893,7 +914,7 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
     if (h->dev.precision != 1) continue;
-    for (int k = 0; k < nsteps; k++) {
+    for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
       h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr);
       mts::launch_tick(h->dev, h->stream);
@@ -903,8 +924,10 @@ mts_status mts_batch_advance(const mts_handle* hs, int32_t n, int32_t nsteps) {
   }
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
-    mts_status s2 = sync_status(h);
-    if (s2 && !st) st = s2;
+    if (h->dev.precision == 1) {
+      mts_status s2 = sync_status(h);
+      if (s2 && !st) st = s2;
+    }
     h->t = t_end[(size_t)i];
   }
   cleanup();

@@ -114,6 +114,7 @@ struct Dev {
   // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
   const double* tsched;
   int* tstep;
+  int tstop;   // batched launches skip the problem once *tstep reaches it
   double* u0;  // the state (every method keeps it here)
   double* u1;  // scratch field
   const long long* mibnode;  // nodes with a MIB flag (any direction), ascending

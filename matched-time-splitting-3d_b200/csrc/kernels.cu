@@ -1194,7 +1194,8 @@ __device__ __forceinline__ SweepIO make_io(const Dev& P, const Roles& r) {
       sdev_[i_] = src_[i_];                                                           \
   }                                                                                   \
   __syncthreads();                                                                    \
-  const Dev& P = *reinterpret_cast<const Dev*>(sdev_);
+  const Dev& P = *reinterpret_cast<const Dev*>(sdev_);                                \
+  if (*P.tstep >= P.tstop) return; /* this problem's steps of the batch are done */
 
 __global__ void __launch_bounds__(TPB) kb_jumps(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items) {
   BATCH_PROLOGUE
@@ -1245,7 +1246,7 @@ __global__ void __launch_bounds__(BNT) kb_sweep(const Dev* __restrict__ Ps, cons
 
 __global__ void kb_tick(const Dev* __restrict__ Ps, int n) {
   const int i = blockIdx.x * TPB + threadIdx.x;
-  if (i < n) ++*Ps[i].tstep;
+  if (i < n && *Ps[i].tstep < Ps[i].tstop) ++*Ps[i].tstep;
 }
 
 template <int D, int KIND>

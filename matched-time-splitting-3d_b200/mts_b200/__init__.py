@@ -18,7 +18,7 @@ import numpy as np
 from ._lib import (CROSSING_DTYPE, EXPORTS, METHODS, MtsError, check, lib_path, load, make_grid, make_params,
                    make_surface)
 
-__all__ = ["Spec", "Solver", "setup_host", "batch_advance", "MtsError", "CROSSING_DTYPE", "METHODS", "EXPORTS", "load", "lib_path"]
+__all__ = ["Spec", "Solver", "setup_host", "batch_advance", "batch_advance_steps", "MtsError", "CROSSING_DTYPE", "METHODS", "EXPORTS", "load", "lib_path"]
 
 
 @dataclass
@@ -73,6 +73,18 @@ def batch_advance(solvers, nsteps: int) -> None:
     L = load()
     arr = (ctypes.c_void_p * len(solvers))(*[s.handle.value for s in solvers])
     check(L.mts_batch_advance(arr, len(solvers), int(nsteps)), "mts_batch_advance")
+
+
+def batch_advance_steps(solvers, counts) -> None:
+    """counts[i] steps of solvers[i], all in one batch
+    (mts_batch_advance_steps)."""
+    solvers = list(solvers)
+    if not solvers:
+        return
+    L = load()
+    arr = (ctypes.c_void_p * len(solvers))(*[s.handle.value for s in solvers])
+    cnt = (ctypes.c_int32 * len(solvers))(*[int(c) for c in counts])
+    check(L.mts_batch_advance_steps(arr, cnt, len(solvers)), "mts_batch_advance_steps")
 
 
 class Solver:

@@ -40,6 +40,7 @@ EXPORTS = [
     "mts_advance",
     "mts_advance_host",
     "mts_batch_advance",
+    "mts_batch_advance_steps",
     "mts_norms",
     "mts_norms_noalloc",
     "mts_get_time",
@@ -161,6 +162,7 @@ def load(build_if_missing: bool = True):
             "mts_advance": [H, ctypes.c_int32],
             "mts_advance_host": [H, vp, vp, ctypes.c_int32],
             "mts_batch_advance": [vp, ctypes.c_int32, ctypes.c_int32],
+            "mts_batch_advance_steps": [vp, vp, ctypes.c_int32],
             "mts_norms": [H, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_norms_noalloc": [H, vp, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_get_time": [H, P(ctypes.c_double)],

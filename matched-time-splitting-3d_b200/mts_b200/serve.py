@@ -7,14 +7,14 @@ Each goes through
      from its grid and crossing count) fits in the HBM budget, then a pool
      thread uploads it (mts_create_from_crossings) and initializes it,
   3. the running batch: at every chunk boundary the server advances all
-     admitted problems together by one mts_batch_advance call (one CUDA graph
-     holding a step of each, replayed), so problems that arrive while others
-     run join the batch as soon as they are uploaded, and their work overlaps
-     on the device,
+     admitted problems together by one mts_batch_advance_steps call (each by
+     up to chunk_steps steps; one launch per kernel of a step for all of
+     them), so problems that arrive while others run join the batch as soon
+     as they are uploaded, and their work overlaps on the device,
   4. retirement: after its last step a problem's error norms are read, its
      device memory is freed and its budget returned.
 Batching does not change any result: each problem's solution is the one it
-gets alone, bit for bit (mts_batch_advance's contract).
+gets alone, bit for bit (mts_batch_advance_steps' contract).
 """
 from __future__ import annotations
 
@@ -24,7 +24,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import Solver, batch_advance, setup_host
+from . import Solver, batch_advance_steps, setup_host
 from .workloads import Request, device_bytes_bound
 
 
@@ -139,10 +139,10 @@ class Server:
                 self.peak_active = max(self.peak_active, len(active))
                 # 4. one chunk of the running batch
                 if active:
-                    k = min(self.chunk, min(j.left for j in active))
-                    batch_advance([j.solver for j in active], k)
+                    ks = [min(self.chunk, j.left) for j in active]
+                    batch_advance_steps([j.solver for j in active], ks)
                     self.batches += 1
-                    for j in active:
+                    for j, k in zip(active, ks):
                         j.left -= k
                     for j in [j for j in active if j.left == 0]:
                         lmax, l2, _ = j.solver.norms()

@@ -67,3 +67,23 @@ def test_batch_rejects_duplicates():
     with M.Solver(sp) as s:
         with pytest.raises(M.MtsError, match="twice"):
             M.batch_advance([s, s], 1)
+
+
+def test_batch_with_per_problem_step_counts():
+    """Problems with different numbers of steps in one batch: each stops at
+    its own count (the server's chunks)."""
+    rng = np.random.default_rng(21)
+    specs = [draw(rng) for _ in range(8)]
+    counts = [int(c) for c in rng.integers(0, 7, len(specs))]
+    solvers = [M.Solver(sp) for sp in specs]
+    try:
+        for s in solvers:
+            s.initialize()
+        M.batch_advance_steps(solvers, counts)
+        for sp, s, c in zip(specs, solvers, counts):
+            u, t = solve_alone(sp, "plain", c)
+            assert s.time == t
+            assert np.array_equal(s.solution(), u), (sp, c)
+    finally:
+        for s in solvers:
+            s.close()

@@ -42,16 +42,16 @@ class FakeSolver:
             self.closed = True
 
 
-def fake_batch(solvers, k):
+def fake_batch(solvers, ks):
     time.sleep(0.001)
-    for s in solvers:
+    for s, k in zip(solvers, ks):
         s.time += k * s.spec.dt
 
 
 @pytest.fixture
 def fakes(monkeypatch):
     monkeypatch.setattr(serve, "Solver", FakeSolver)
-    monkeypatch.setattr(serve, "batch_advance", fake_batch)
+    monkeypatch.setattr(serve, "batch_advance_steps", fake_batch)
     monkeypatch.setattr(serve, "setup_host", lambda spec: (None, np.zeros(4), None))
     monkeypatch.setattr(serve, "device_bytes_bound", lambda spec, nc: 100)
     FakeSolver.live = FakeSolver.peak = 0
