@@ -422,9 +422,11 @@ __device__ __forceinline__ double source_from(const Dev& P, double S, double R2,
 // Shared memory of a shape: the staging ring, the two prefix factor tables
 // of the sweep direction (2 sides x 2 values x n rows) and its exact-solution
 // tables (3 x n).
-template <int CH, int NS, int NT>
+template <int CH, int NS, int NT, int D = 0>
 constexpr size_t shape_smem(int n) {
-  return sizeof(double) * ((size_t)3 * NS * CH * NT + (size_t)7 * n);
+  // D = 0 pads each ring row by 4 doubles (the x sweeps' cooperative staging);
+  // the default D = 0 is the largest, used for the fit check
+  return sizeof(double) * ((size_t)3 * NS * CH * (D == 0 ? NT + 4 : NT) + (size_t)7 * n);
 }
 
 
@@ -433,15 +435,19 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
   static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4, "shape");
   static_assert(CH <= kRowPad, "chunk rows past a line end must stay within the fields' slack");
   constexpr int RING = NS * CH;    // rows in a field's ring
-  constexpr int SLOT = CH * NT;    // doubles per chunk slot
+  // x lines (kCoop, below) are staged by the warp together, with 4 doubles of
+  // padding per ring row so that a copy instruction's lanes, which write
+  // CH rows of 32/CH columns, fall on distinct banks in pairs
+  constexpr int RS = D == 0 ? NT + 4 : NT;  // doubles per ring row
+  constexpr int SLOT = CH * RS;    // doubles per chunk slot
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
   double* const sA = sm + tid;             // [NS][CH][NT]
   double* const sB = sA + NS * SLOT;       // [NS][CH][NT]
   double* const sC = sB + NS * SLOT;       // [NS][CH][NT]
-#define SA(j) sA[((j) & (RING - 1)) * NT]
-#define SB(j) sB[((j) & (RING - 1)) * NT]
-#define SC(j) sC[((j) & (RING - 1)) * NT]
+#define SA(j) sA[((j) & (RING - 1)) * RS]
+#define SB(j) sB[((j) & (RING - 1)) * RS]
+#define SC(j) sC[((j) & (RING - 1)) * RS]
   const long long T = (long long)ncta_ * NT;
   const long long gt = (long long)cta_ * NT + tid;
   double* const dp = P.dp + gt;
@@ -472,14 +478,28 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
   }
   __syncthreads();
 
-  for (long long t = gt; t < nl; t += T) {
+  // x lines are contiguous in memory and 2 KB apart, so a thread staging its
+  // own line would touch 32 segments per warp instruction.  There the warp
+  // stages and stores its 32 lines together (kCoop): lane e of copy q moves
+  // row e % CH of line e / CH, so runs of CH lanes read one line's
+  // consecutive rows, into that line's column of the ring.  The warp then
+  // walks its lines' chunks in step, including lanes whose line is a face
+  // line or past the end, which only help with the copies.
+  constexpr bool kCoop = D == 0;
+  const int lane = tid & 31;
+  double* const sAw = sm + (tid - lane);  // the warp's first column of ring A
+  const long long nxl = P.nx;
+
+  for (long long t0 = gt - (kCoop ? lane : 0); t0 < nl; t0 += T) {
+    const long long t = kCoop ? t0 + lane : t0;
+    const bool act = t < nl;
     Line L;
-    decode_line<D>(P, t, L);
+    decode_line<D>(P, act ? t : nl - 1, L);
     const int n = L.n;
     const long long s = L.s;
     LineExact fx;
     line_exact<D>(P, L, fx);
-    if (L.boundary) {
+    if (L.boundary && act) {
       if (io.bmode) {
         for (int j = 0; j < n; j++) {
           long long m = L.base + (long long)j * s;
@@ -490,7 +510,14 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
           io.out[m] = v;
         }
       }
-      continue;
+    }
+    const bool solve = act && !L.boundary;
+    if (!kCoop && !solve) continue;
+    unsigned solvers = 0;
+    if (kCoop) {
+      __syncwarp();
+      solvers = __ballot_sync(0xffffffffu, solve);
+      if (!solvers) continue;
     }
     const int nch = (n + CH - 1) / CH;
     const int ls = P.lside[D][L.lid];
@@ -504,21 +531,52 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
     const double* gA = (KIND == K_COPY ? io.add : io.stin) + L.base;
     const double* gB = io.add + L.base;
     const double* gC = fbet + L.base;
+    // kCoop: the first MIB row of the line each of this lane's copies serves
+    int L1q[CH];
+    long long gq[CH];  // start of the line each copy serves, or -1 past the end
+    if (kCoop) {
+#pragma unroll
+      for (int q = 0; q < CH; q++) {
+        const int l = (q * 32 + lane) / CH;
+        L1q[q] = __shfl_sync(0xffffffffu, L1, l);
+        gq[q] = t0 + l < nl ? (t0 + l) * nxl + (q * 32 + lane) % CH : -1;
+      }
+    }
     auto stage = [&](int c) {
+      if (kCoop) {
+        if (c < nch) {
+          const double* fA = KIND == K_COPY ? io.add : io.stin;
+          double* aw = sAw + (c & (NS - 1)) * SLOT;
+          double* bw = aw + NS * SLOT;
+          double* cw = bw + NS * SLOT;
+#pragma unroll
+          for (int q = 0; q < CH; q++) {
+            const int e = q * 32 + lane, l = e / CH, r = e % CH;
+            if (gq[q] >= 0) {
+              const long long g = gq[q] + (long long)c * CH;
+              cp_async8(aw + r * RS + l, fA + g);
+              if (two) cp_async8(bw + r * RS + l, io.add + g);
+              if ((c + 1) * CH > L1q[q] && L1q[q] < n) cp_async8(cw + r * RS + l, fbet + g);
+            }
+          }
+        }
+        cp_async_commit();
+        return;
+      }
       if (c < nch) {
         const long long off = (long long)c * CH * s;
         double* a = sA + (c & (NS - 1)) * SLOT;
 #pragma unroll
-        for (int r = 0; r < CH; r++) cp_async8(a + r * NT, gA + off + r * s);
+        for (int r = 0; r < CH; r++) cp_async8(a + r * RS, gA + off + r * s);
         if (two) {
           double* b = sB + (c & (NS - 1)) * SLOT;
 #pragma unroll
-          for (int r = 0; r < CH; r++) cp_async8(b + r * NT, gB + off + r * s);
+          for (int r = 0; r < CH; r++) cp_async8(b + r * RS, gB + off + r * s);
         }
-        if ((c + 1) * CH > L1) {
+        if ((c + 1) * CH > L1 && L1 < n) {  // per-node factors exist only for lines with blocks
           double* cc = sC + (c & (NS - 1)) * SLOT;
 #pragma unroll
-          for (int r = 0; r < CH; r++) cp_async8(cc + r * NT, gC + off + r * s);
+          for (int r = 0; r < CH; r++) cp_async8(cc + r * RS, gC + off + r * s);
         }
       }
       cp_async_commit();
@@ -557,8 +615,13 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
     double dprev = 0.0;
     int j = 1;
     for (int c = 0; c < nch; c++) {
+      if (kCoop) __syncwarp();  // every lane is done with the slot restaged next
       stage(c + NS - 2);
       cp_async_wait<NS - 3>();  // chunks c-1, c, c+1 resident
+      if (kCoop) {
+        __syncwarp();  // and the other lanes' copies into this lane's column visible
+        if (!solve) continue;
+      }
       if (c == 0) {
         dprev = outer_at(0) / pt[0];
         dp[0] = dprev;
@@ -579,13 +642,13 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
           // tag: bet from the staged per-node factors, else from the prefix table
           constexpr bool kField = decltype(tag)::value;
           const double* bt = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0;
-          double xm = ap[(CH - 1) * NT];
+          double xm = ap[(CH - 1) * RS];
           double x0 = a[0];
 #pragma unroll
           for (int rr = 0; rr < CH; rr++) {
-            const double xp = rr == CH - 1 ? an[0] : a[(rr + 1) * NT];
-            const double r = rhs(c0 + rr, xm, x0, xp, two ? b[rr * NT] : x0, w0, w1, w2, mside);
-            const double bet = kField ? bt[rr * NT] : bt[2 * rr];
+            const double xp = rr == CH - 1 ? an[0] : a[(rr + 1) * RS];
+            const double r = rhs(c0 + rr, xm, x0, xp, two ? b[rr * RS] : x0, w0, w1, w2, mside);
+            const double bet = kField ? bt[rr * RS] : bt[2 * rr];
             const double d = (r - ac * dprev) / bet;
             q[rr * T] = d;
             dprev = d;
@@ -631,7 +694,7 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
         }
       }
     }
-    {
+    if (solve) {
       // last row: the Dirichlet identity row (a = 0)
       const double r = outer_at(n - 1);
       const double a = 0.0;
@@ -651,12 +714,12 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
         double* a = sA + (c & (NS - 1)) * SLOT;
         const double* g = dp + (long long)c * CH * T;
 #pragma unroll
-        for (int r = 0; r < CH; r++) cp_async8(a + r * NT, g + r * T);
-        if ((c + 1) * CH >= L1) {
+        for (int r = 0; r < CH; r++) cp_async8(a + r * RS, g + r * T);
+        if ((c + 1) * CH >= L1 && L1 < n) {
           double* b = sB + (c & (NS - 1)) * SLOT;
           const long long off = ((long long)c * CH + 1) * s;
 #pragma unroll
-          for (int r = 0; r < CH; r++) cp_async8(b + r * NT, gG + off + r * s);
+          for (int r = 0; r < CH; r++) cp_async8(b + r * RS, gG + off + r * s);
         }
       }
       cp_async_commit();
@@ -671,12 +734,17 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
     double unext = 0.0;
     for (int c = nch - 1; c > nch - NS; c--) bstage(c);
     for (int c = nch - 1; c >= 0; c--) {
+      if (kCoop) __syncwarp();  // the previous chunk's stores have read its slot
       bstage(c - NS + 1);
       cp_async_wait<NS - 1>();
       const int c0 = c * CH;
-      if (!io.last && c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
+      // kCoop: results go to this lane's column of the slot, then the warp
+      // stores its lines' rows together
+      double* const aslot = sA + (c & (NS - 1)) * SLOT;
+      if (!solve) {
+      } else if (!io.last && c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
         // every row has a successor; gam_{j+1} from one source
-        const double* a = sA + (c & (NS - 1)) * SLOT;
+        double* a = aslot;
         double* o = io.out + L.base + (long long)c0 * s;
         auto run = [&](auto tag) {
           // tag: gam_{j+1} from the staged per-node factors, else from the
@@ -685,11 +753,14 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
           const double* gb = kField ? sB + (c & (NS - 1)) * SLOT : pt + 2 * c0 + 3;
 #pragma unroll
           for (int rr = CH - 1; rr >= 0; rr--) {
-            const double gm = kField ? gb[rr * NT] : gb[2 * rr];
-            double u = a[rr * NT];
+            const double gm = kField ? gb[rr * RS] : gb[2 * rr];
+            double u = a[rr * RS];
             u -= gm * unext;
             unext = u;
-            o[rr * s] = u;
+            if (kCoop)
+              a[rr * RS] = u;
+            else
+              o[rr * s] = u;
           }
         };
         if (c0 + 1 >= L1)
@@ -731,7 +802,19 @@ __device__ __forceinline__ void k_sweep_body(const Dev& P, unsigned cta_, unsign
             row_parts<D>(fx, sX, nd, jj, S, R2);
             v = u + P.dt * source_from(P, S, R2, E1, side);
           }
-          io.out[L.base + (long long)jj * s] = v;
+          if (kCoop)
+            SA(jj) = v;
+          else
+            io.out[L.base + (long long)jj * s] = v;
+        }
+      }
+      if (kCoop) {
+        __syncwarp();
+        const double* aw = sAw + (c & (NS - 1)) * SLOT;
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+          const int e = q * 32 + lane, l = e / CH, r = e % CH;
+          if (((solvers >> l) & 1u) && c0 + r < n) io.out[gq[q] + c0] = aw[r * RS + l];
         }
       }
     }
@@ -861,7 +944,7 @@ template <int D, int KIND, int CH, int NS, int NT>
 void sweep_shape(const Dev& P, const SweepIO& io, cudaStream_t st) {
   // persistent CTAs, one per SM at most, no more than the lines need
   const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
-  k_sweep<D, KIND, CH, NS, NT><<<sweep_grid(P, nlines<D>(P), NT), NT, shape_smem<CH, NS, NT>(nd), st>>>(P, io);
+  k_sweep<D, KIND, CH, NS, NT><<<sweep_grid(P, nlines<D>(P), NT), NT, shape_smem<CH, NS, NT, D>(nd), st>>>(P, io);
 }
 
 template <int D, int KIND>
@@ -1256,7 +1339,7 @@ void bsweep(const BatchPlan& b, const Roles& r, cudaStream_t st, int& launches) 
     launches++;
   }
   if (b.nsw[D] > 0) {
-    kb_sweep<D, KIND><<<b.nsw[D], BNT, shape_smem<BCH, BNS, BNT>(b.nmax), st>>>(b.Ps, b.sw[D], r);
+    kb_sweep<D, KIND><<<b.nsw[D], BNT, shape_smem<BCH, BNS, BNT, D>(b.nmax), st>>>(b.Ps, b.sw[D], r);
     launches++;
   }
 }

@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
         float* a = sA + (c & (NS - 1)) * SLOT;
 #pragma unroll
         for (int r = 0; r < CH; r++) cp_async4(a + r * NT, gA + off + r * s);
-        if ((c + 1) * CH > L1) {
+        if ((c + 1) * CH > L1 && L1 < n) {  // per-node factors exist only for lines with blocks
           float* cc = sC + (c & (NS - 1)) * SLOT;
 #pragma unroll
           for (int r = 0; r < CH; r++) cp_async4(cc + r * NT, gC + off + r * s);
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
         const float* g = dp + (long long)c * CH * T;
 #pragma unroll
         for (int r = 0; r < CH; r++) cp_async4(a + r * NT, g + r * T);
-        if ((c + 1) * CH >= L1) {
+        if ((c + 1) * CH >= L1 && L1 < n) {
           float* b = sC + (c & (NS - 1)) * SLOT;
           const long long off = ((long long)c * CH + 1) * s;
 #pragma unroll
