@@ -201,7 +201,8 @@ __device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
 // (2 sides x 2 values x n rows), all FP32.
 template <int CH, int NS, int NT>
 constexpr size_t shape32_smem(int n) {
-  return sizeof(float) * ((size_t)2 * NS * CH * NT + (size_t)4 * n);
+  // x sweeps pad each ring row by 4 floats; the size covers that case
+  return sizeof(float) * ((size_t)2 * NS * CH * (NT + 4) + (size_t)4 * n);
 }
 
 // One thread per line, persistent CTAs, as the FP64 sweep (kernels.cu): f
@@ -212,13 +213,18 @@ template <int D, int CH, int NS, int NT>
 __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P, float* f) {
   static_assert((CH & (CH - 1)) == 0 && (NS & (NS - 1)) == 0 && NS >= 4 && CH >= 4 && CH <= kRowPad, "shape");
   constexpr int RING = NS * CH;
-  constexpr int SLOT = CH * NT;
+  // x lines are staged and stored by the warp together (as in the FP64 sweep),
+  // with 4 floats of padding per ring row so that a copy's lanes (CH rows of
+  // 32/CH columns) fall on 32 distinct banks
+  constexpr bool kCoop = D == 0;
+  constexpr int RS = kCoop ? NT + 4 : NT;  // floats per ring row
+  constexpr int SLOT = CH * RS;
   extern __shared__ float sm32[];
   const int tid = threadIdx.x;
   float* const sA = sm32 + tid;
   float* const sC = sA + NS * SLOT;
-#define RA(j) sA[((j) & (RING - 1)) * NT]
-#define RC(j) sC[((j) & (RING - 1)) * NT]
+#define RA(j) sA[((j) & (RING - 1)) * RS]
+#define RC(j) sC[((j) & (RING - 1)) * RS]
   const long long T = (long long)gridDim.x * NT;
   const long long gt = (long long)blockIdx.x * NT + tid;
   float* const dp = P.dp32 + gt;
@@ -232,13 +238,25 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
   float* const sP = sm32 + 2 * NS * SLOT;
   for (int i = tid; i < 4 * nd; i += NT) sP[i] = i < 2 * nd ? P.ptab32[D][0][i] : P.ptab32[D][1][i - 2 * nd];
   __syncthreads();
+  const int lane = tid & 31;
+  float* const sAw = sm32 + (tid - lane);  // the warp's first column of ring A
+  const long long nxl = P.nx;
 
-  for (long long t = gt; t < nl; t += T) {
+  for (long long t0 = gt - (kCoop ? lane : 0); t0 < nl; t0 += T) {
+    const long long t = kCoop ? t0 + lane : t0;
+    const bool act = t < nl;
     Line L;
-    decode_line<D>(P, t, L);
+    decode_line<D>(P, act ? t : nl - 1, L);
     const int n = L.n;
     const long long s = L.s;
-    if (L.boundary) continue;  // face line: the solution is the right-hand side itself
+    // face line: the solution is the right-hand side itself
+    const bool solve = act && !L.boundary;
+    if (!kCoop && !solve) continue;
+    unsigned solvers = 0;
+    if (kCoop) {
+      solvers = __ballot_sync(0xffffffffu, solve);
+      if (!solvers) continue;
+    }
     const int nch = (n + CH - 1) / CH;
     const int ls = P.lside[D][L.lid];
     const int bfirst = P.bstart[D][L.lid];
@@ -247,16 +265,43 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
     const float* pt = sP + ((ls >> 1) & 1) * 2 * nd;
     const float* gA = f + L.base;
     const float* gC = fib + L.base;
+    int L1q[CH];
+    long long gq[CH];  // start of the line each cooperative copy serves, -1 past the end
+    if (kCoop) {
+#pragma unroll
+      for (int q = 0; q < CH; q++) {
+        const int l = (q * 32 + lane) / CH;
+        L1q[q] = __shfl_sync(0xffffffffu, L1, l);
+        gq[q] = t0 + l < nl ? (t0 + l) * nxl + (q * 32 + lane) % CH : -1;
+      }
+    }
     auto stage = [&](int c) {
+      if (kCoop) {
+        if (c < nch) {
+          float* aw = sAw + (c & (NS - 1)) * SLOT;
+          float* cw = aw + NS * SLOT;
+#pragma unroll
+          for (int q = 0; q < CH; q++) {
+            const int e = q * 32 + lane, l = e / CH, r = e % CH;
+            if (gq[q] >= 0) {
+              const long long g = gq[q] + (long long)c * CH;
+              cp_async4(aw + r * RS + l, f + g);
+              if ((c + 1) * CH > L1q[q] && L1q[q] < n) cp_async4(cw + r * RS + l, fib + g);
+            }
+          }
+        }
+        cp_async_commit();
+        return;
+      }
       if (c < nch) {
         const long long off = (long long)c * CH * s;
         float* a = sA + (c & (NS - 1)) * SLOT;
 #pragma unroll
-        for (int r = 0; r < CH; r++) cp_async4(a + r * NT, gA + off + r * s);
+        for (int r = 0; r < CH; r++) cp_async4(a + r * RS, gA + off + r * s);
         if ((c + 1) * CH > L1 && L1 < n) {  // per-node factors exist only for lines with blocks
           float* cc = sC + (c & (NS - 1)) * SLOT;
 #pragma unroll
-          for (int r = 0; r < CH; r++) cp_async4(cc + r * NT, gC + off + r * s);
+          for (int r = 0; r < CH; r++) cp_async4(cc + r * RS, gC + off + r * s);
         }
       }
       cp_async_commit();
@@ -272,8 +317,13 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
     float dprev = 0.0f;
     int j = 1;
     for (int c = 0; c < nch; c++) {
+      if (kCoop) __syncwarp();  // every lane is done with the slot restaged next
       stage(c + NS - 2);
       cp_async_wait<NS - 3>();
+      if (kCoop) {
+        __syncwarp();  // the other lanes' copies into this lane's column are visible
+        if (!solve) continue;
+      }
       if (c == 0) {
         dprev = RA(0) * pt[0];
         dp[0] = dprev;
@@ -290,8 +340,8 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
           const float* bt = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0;
 #pragma unroll
           for (int rr = 0; rr < CH; rr++) {
-            const float ib = kField ? bt[rr * NT] : bt[2 * rr];
-            const float d = __fmul_rn(__fmaf_rn(-ac, dprev, a[rr * NT]), ib);
+            const float ib = kField ? bt[rr * RS] : bt[2 * rr];
+            const float d = __fmul_rn(__fmaf_rn(-ac, dprev, a[rr * RS]), ib);
             q[rr * T] = d;
             dprev = d;
           }
@@ -328,7 +378,7 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
         }
       }
     }
-    {
+    if (solve) {
       // last row: the Dirichlet identity row (a = 0)
       const float ib = n - 1 >= L1 ? RC(n - 1) : pt[2 * (n - 1)];
       dp[(long long)(n - 1) * T] = __fmul_rn(RA(n - 1), ib);
@@ -343,12 +393,12 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
         float* a = sA + (c & (NS - 1)) * SLOT;
         const float* g = dp + (long long)c * CH * T;
 #pragma unroll
-        for (int r = 0; r < CH; r++) cp_async4(a + r * NT, g + r * T);
+        for (int r = 0; r < CH; r++) cp_async4(a + r * RS, g + r * T);
         if ((c + 1) * CH >= L1 && L1 < n) {
           float* b = sC + (c & (NS - 1)) * SLOT;
           const long long off = ((long long)c * CH + 1) * s;
 #pragma unroll
-          for (int r = 0; r < CH; r++) cp_async4(b + r * NT, gG + off + r * s);
+          for (int r = 0; r < CH; r++) cp_async4(b + r * RS, gG + off + r * s);
         }
       }
       cp_async_commit();
@@ -356,20 +406,25 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
     float xnext = 0.0f;
     for (int c = nch - 1; c > nch - NS; c--) bstage(c);
     for (int c = nch - 1; c >= 0; c--) {
+      if (kCoop) __syncwarp();  // the previous chunk's stores have read its slot
       bstage(c - NS + 1);
       cp_async_wait<NS - 1>();
       const int c0 = c * CH;
-      if (c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
-        const float* a = sA + (c & (NS - 1)) * SLOT;
+      if (!solve) {
+      } else if (c0 + CH <= n - 1 && (c0 + CH < L1 || c0 + 1 >= L1)) {
+        float* a = sA + (c & (NS - 1)) * SLOT;
         auto run = [&](auto tag) {
           constexpr bool kField = decltype(tag)::value;
           const float* gb = kField ? sC + (c & (NS - 1)) * SLOT : pt + 2 * c0 + 3;
 #pragma unroll
           for (int rr = CH - 1; rr >= 0; rr--) {
-            const float gm = kField ? gb[rr * NT] : gb[2 * rr];
-            const float x = __fmaf_rn(-gm, xnext, a[rr * NT]);
+            const float gm = kField ? gb[rr * RS] : gb[2 * rr];
+            const float x = __fmaf_rn(-gm, xnext, a[rr * RS]);
             xnext = x;
-            f[L.base + (long long)(c0 + rr) * s] = x;
+            if (kCoop)
+              a[rr * RS] = x;
+            else
+              f[L.base + (long long)(c0 + rr) * s] = x;
           }
         };
         if (c0 + 1 >= L1)
@@ -383,7 +438,19 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
           float x = RA(jj);
           if (jj != n - 1) x = __fmaf_rn(-(jj + 1 >= L1 ? RC(jj) : pt[2 * (jj + 1) + 1]), xnext, x);
           xnext = x;
-          f[L.base + (long long)jj * s] = x;
+          if (kCoop)
+            RA(jj) = x;
+          else
+            f[L.base + (long long)jj * s] = x;
+        }
+      }
+      if (kCoop) {
+        __syncwarp();
+        const float* aw = sAw + (c & (NS - 1)) * SLOT;
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+          const int e = q * 32 + lane, l = e / CH, r = e % CH;
+          if (((solvers >> l) & 1u) && c0 + r < n) f[gq[q] + c0] = aw[r * RS + l];
         }
       }
     }
@@ -393,7 +460,6 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
 #undef RC
 }
 
-// Shapes of the FP32 sweep (rows per chunk, ring chunks, threads per CTA).
 // Shape of the FP32 sweeps (rows per chunk, ring chunks, threads per CTA):
 // 448 threads on each of the 148 SMs cover the 66,049 lines of a 257^3 grid
 // in one wave.
