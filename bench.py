@@ -327,6 +327,25 @@ def auto_procs(w) -> int:
 
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(values, dist=None):
+    """Element-wise max of per-rank timings over all ranks (every rank takes
+    part; a device tensor under NCCL, a host tensor under gloo)."""
+    import torch
+
+    if dist is None:
+        return [float(v) for v in values]
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(list(values), dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_value(world: int, nodes: int, steps: int, ms_max: float) -> float:
+    """Whole-job throughput: every rank advances its own replica of `nodes`
+    cells by `steps` steps; the job takes the slowest rank's time."""
+    return world * nodes * steps / (ms_max / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -441,12 +460,9 @@ def main():
     solver.synchronize()
     e2e_ms = e0.elapsed_time(e1)
 
-    t_all = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
-    ms_max, e2e_max = float(t_all[0]), float(t_all[1])
-    value = world * nodes * a.steps / (ms_max / 1e3)
-    e2e_value = world * nodes * e2e_steps / (e2e_max / 1e3)
+    ms_max, e2e_max = max_over_ranks([ms, e2e_ms], dist)
+    value = job_value(world, nodes, a.steps, ms_max)
+    e2e_value = job_value(world, nodes, e2e_steps, e2e_max)
 
     # The mixed-precision form (FP32 line solves on the increment, FP64
     # residual and state) on the same workload, same steps from the same
@@ -479,11 +495,8 @@ def main():
         assert sm.time == t_plain
         sm.close()
         del um
-        tm = torch.tensor([ms_m], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ms_m = float(tm[0])
-        v_m = world * nodes * a.steps / (ms_m / 1e3)
+        (ms_m,) = max_over_ranks([ms_m], dist)
+        v_m = job_value(world, nodes, a.steps, ms_m)
         names_m = ["jumps", "residual_fp64", "x_sweep_fp32", "y_sweep_fp32", "z_sweep_fp32_and_accumulate"]
         mixed = {
             "value": v_m, "unit": "cell-steps/s", "ms_per_step": ms_m / a.steps,

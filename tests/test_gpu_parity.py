@@ -139,3 +139,51 @@ def test_every_sweep_shape_gives_the_oracle_bits(method):
             assert np.array_equal(u, u_or), f"shape {shape}: rel {rel_maxdiff(u, u_or):.3e}"
             tried += 1
     assert tried >= 6
+
+
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+@pytest.mark.parametrize("mib", [1, 2])
+@pytest.mark.parametrize("surface", ["ellipsoid", "torus"])
+def test_gpu_matches_oracle_129(method, mib, surface):
+    """The 129^3 grid of the drop-in configuration (beta 1:1000, dt = h),
+    every method and MIB variant, 2 steps, GPU vs oracle bit for bit."""
+    n = (129, 129, 129)
+    sp = (0.7001, 0.4999, 0.4001, 1.0) if surface == "ellipsoid" else (0.5, 0.2)
+    spec = M.Spec(n=n, surface=surface, surface_params=sp, beta_in=1.0, beta_out=1000.0, method=method, mib=mib,
+                  dt=2.0 / 128)
+    tags, cr, _ = M.setup_host(spec)
+    prob = O.Problem(n=n, surface=surface, surface_params=sp, beta_in=1.0, beta_out=1000.0, method=method, mib=mib,
+                     dt=2.0 / 128, steps=2)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    u, _, _ = run_gpu(spec, 2)
+    assert rel_maxdiff(u, u_or) <= TOL
+    assert np.array_equal(u, u_or)
+
+
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+def test_gpu_matches_oracle_257(method):
+    """The bench's 257^3 grid (torus, MIB-L2, beta 1:1000, dt = h), 2 steps of
+    every method, GPU vs oracle bit for bit."""
+    n = (257, 257, 257)
+    spec = M.Spec(n=n, surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, method=method,
+                  mib=2, dt=2.0 / 256)
+    tags, cr, _ = M.setup_host(spec)
+    prob = O.Problem(n=n, surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, method=method,
+                     mib=2, dt=2.0 / 256, steps=2)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    u, (lmax, l2, am), t = run_gpu(spec, 2)
+    assert rel_maxdiff(u, u_or) <= TOL
+    assert np.array_equal(u, u_or)
+    lo, l2o, amo = O.port_norms(prob, tags, t, u_or)
+    assert lmax == lo and tuple(am) == amo
+
+
+def test_eq0_constant_solution_is_kept_at_257():
+    """A size-independent property at the full size: with Eq_0 (constant
+    solutions 80 inside, 100 outside, zero source, jumps [u] = 20) the scheme
+    keeps the exact solution to rounding, as the reference does (its Eq_0
+    error is 4e-12 at 33^3)."""
+    spec = M.Spec(n=(257, 257, 257), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0,
+                  eq=0, method="adi", mib=2, dt=2.0 / 256)
+    u, (lmax, l2, _), _ = run_gpu(spec, 3)
+    assert lmax <= 1e-9 * 100.0, lmax
