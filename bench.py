@@ -87,12 +87,67 @@ def parse():
     ap.add_argument("--served-requests", type=int, default=1000,
                     help="requests per arrival rate (the full served workload is 10000)")
     ap.add_argument("--served-rates", default="200,1000", help="Poisson arrival rates, requests/s")
+    ap.add_argument("--workload", default="step", choices=["step", "precision", "batched", "served"],
+                    help="step: the headline line (default); precision / batched / served: the full sweep of "
+                         "that form alone, one JSON line")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------
 # Batched and served forms (wall-clock: the unit is whole solves, setup of the
 # device state and host work included; the GPU is synchronized at both ends).
+
+def run_precision(grids=(257, 385), betas=(1e-3, 1.0, 1e3), steps: int = 20) -> dict:
+    """The precision form against the plain form: Douglas-ADI + MIB-L2, torus,
+    beta_out / beta_in in `betas`, dt = h, `steps` steps of each from the same
+    start; cell-steps/s of both (CUDA events), L-infinity of both against the
+    exact solution, and the mixed solution's difference from the plain one."""
+    import numpy as np
+    import torch
+
+    import mts_b200 as M
+
+    out = {}
+    for n in grids:
+        for b in betas:
+            spec = M.Spec(n=(n, n, n), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=b,
+                          method="adi", mib=2, dt=2.0 / (n - 1))
+            res = {}
+            for prec in ("plain", "mixed"):
+                with M.Solver(spec) as s:
+                    s.set_precision(prec)
+                    if prec == "plain":
+                        s.autotune(1)
+                    s.initialize()
+                    s.advance(2)
+                    s.synchronize()
+                    s.time = 0.0
+                    s.initialize()
+                    st = torch.cuda.ExternalStream(s.stream())
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    s.advance(steps)
+                    e1.record(st)
+                    s.synchronize()
+                    ms = e0.elapsed_time(e1)
+                    lmax, l2, _ = s.norms()
+                    res[prec] = (ms, lmax, l2, s.solution())
+            up, um = res["plain"][3], res["mixed"][3]
+            nodes = n ** 3
+            out[f"{n}^3 beta {b:g}"] = {
+                "plain_cell_steps_per_s": nodes * steps / (res["plain"][0] / 1e3),
+                "mixed_cell_steps_per_s": nodes * steps / (res["mixed"][0] / 1e3),
+                "speedup": res["plain"][0] / res["mixed"][0],
+                "linf_exact_plain": res["plain"][1], "linf_exact_mixed": res["mixed"][1],
+                "linf_ratio": res["mixed"][1] / res["plain"][1],
+                "linf_vs_plain_fp64": float(np.abs(um - up).max()),
+                "rel_maxdiff_vs_plain": float(np.abs(um - up).max() / np.abs(up).max()),
+            }
+            del up, um, res
+    return {"workload": "precision form: 257^3 and 385^3 Douglas-ADI MIB-L2 torus, beta 1e-3/1/1e3, dt = h, "
+                        f"{steps} steps", "steps": steps, "cases": out}
+
 
 def run_batched(count: int, steps: int, seed: int = 0) -> dict:
     """`count` independent problems of the batched family, `steps` steps each:
@@ -358,6 +413,22 @@ def main():
     world, rank, local = dist_setup()
     w = workload(a)
     nodes = w["n"][0] * w["n"][1] * w["n"][2]
+
+    if a.workload != "step":
+        # one form's full workload on one GPU, one JSON line (rank 0 only)
+        if rank != 0:
+            return 0
+        import torch
+
+        torch.cuda.set_device(local)
+        if a.workload == "precision":
+            res = run_precision()
+        elif a.workload == "batched":
+            res = run_batched(a.batch_problems, a.batch_steps)
+        else:
+            res = run_served(a.served_requests, [float(v) for v in a.served_rates.split(",") if v])
+        print(json.dumps({"workload": a.workload, **res}))
+        return 0
 
     if a.impl == "reference":
         if rank != 0:

@@ -35,11 +35,16 @@ mts_status fail(mts_status s, const std::string& msg) {
     }                                                                              \
   } while (0)
 
+// Device memory comes from the device's stream-ordered pool (cudaMallocAsync
+// on the handle's stream, cudaFreeAsync when the handle is destroyed): a
+// server that creates and destroys problems continuously then neither
+// synchronizes the device on every free nor returns memory to the driver in
+// between (the pool keeps what it has, see configure_pool).
 template <class T>
 cudaError_t upload(T** dst, const T* src, size_t n, cudaStream_t st) {
   *dst = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
+  cudaError_t e = cudaMallocAsync((void**)dst, n * sizeof(T), st);
   if (e != cudaSuccess) return e;
   if (src) return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st);
   return cudaSuccess;
@@ -64,7 +69,7 @@ struct mts_problem {
   int64_t device_bytes = 0;  // sum of the allocations' sizes
   double* norm_part = nullptr;
   double* norm_out = nullptr;
-  double* host_norm = nullptr;  // pinned, 3 doubles
+
   int norm_nb = 1;
   double t = 0;
   int64_t launches = 0;
@@ -82,9 +87,11 @@ struct mts_problem {
       for (cudaEvent_t e : a) cudaEventDestroy(e);
     for (auto& a : ev_free)
       for (cudaEvent_t e : a) cudaEventDestroy(e);
-    for (void* p : allocations) cudaFree(p);
-    if (host_norm) cudaFreeHost(host_norm);
-    if (stream) cudaStreamDestroy(stream);
+    for (void* p : allocations) cudaFreeAsync(p, stream);
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
   }
   template <class T>
   cudaError_t put(T** dst, const T* src, size_t n) {
@@ -443,6 +450,17 @@ mts_status finish_create(mts_problem* h) {
     }
   }
 
+  // the device's pool keeps freed memory for the next allocations instead of
+  // returning it to the driver at every synchronization (once per device)
+  static bool pool_kept[64] = {};
+  if (h->device >= 0 && h->device < 64 && !pool_kept[h->device]) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pool_kept[h->device] = true;
+  }
   static bool configured = false;
   if (!configured) {
     mts::configure_kernels();
@@ -574,7 +592,6 @@ mts_status finish_create(mts_problem* h) {
   h->norm_nb = mts::norms_blocks(D);
   CUDA_TRY(h->put(&h->norm_part, (const double*)nullptr, (size_t)3 * h->norm_nb));
   CUDA_TRY(h->put(&h->norm_out, (const double*)nullptr, 3));
-  CUDA_TRY(cudaMallocHost((void**)&h->host_norm, 3 * sizeof(double)));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->t = p.t0;
   return MTS_OK;
@@ -801,7 +818,7 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
   mts_status st = MTS_OK;
   auto cleanup = [&]() {
     for (cudaStream_t q : streams) cudaStreamDestroy(q);
-    for (void* q : dev_alloc) cudaFree(q);
+    for (void* q : dev_alloc) cudaFreeAsync(q, hs[0]->stream);
     for (int i = 0; i < n; i++) {
       hs[i]->dev.tsched = nullptr;
       hs[i]->dev.tstep = nullptr;
@@ -819,7 +836,7 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
   } while (0)
   auto dev_upload = [&](const void* src, size_t bytes, cudaStream_t q, void** out) -> cudaError_t {
     *out = nullptr;
-    cudaError_t e = cudaMalloc(out, bytes ? bytes : 16);
+    cudaError_t e = cudaMallocAsync(out, bytes ? bytes : 16, q);
     if (e != cudaSuccess) return e;
     dev_alloc.push_back(*out);
     return bytes ? cudaMemcpyAsync(*out, src, bytes, cudaMemcpyHostToDevice, q) : cudaSuccess;
@@ -949,9 +966,9 @@ mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3) {
   if (!h) return fail(MTS_ERR_ARG, "null handle");
   h->launches += mts::launch_norms(h->dev, std::exp(-h->t), h->u0, h->norm_part, h->norm_nb, h->norm_out, h->stream);
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(h->host_norm, h->norm_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  double r[3];
+  CUDA_TRY(cudaMemcpyAsync(r, h->norm_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   mts_status st = sync_status(h);
-  const double* r = h->host_norm;
   if (lmax) *lmax = r[0];
   if (l2) *l2 = r[2];
   if (argmax3) {
