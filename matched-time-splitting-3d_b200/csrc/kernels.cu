@@ -97,69 +97,69 @@ __device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __rest
 }
 
 template <int G>
-__device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ un, double* __restrict__ R, double E) {
+__device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_,
+                                               const double* __restrict__ un, double* __restrict__ R, double E) {
   E = step_e(P, E, 2);
-  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
-  const int nrows = P.ny * P.nz;
+  const int nx = P.nx, nrows = P.ny * P.nz;
+  const long long sy = nx, sz = (long long)nx * P.ny;
   const double dt = P.dt;
-  // regular 3-point weights by side, in registers
-  const double y0i = P.vd[1][0][0], y1i = P.vd[1][0][1], y2i = P.vd[1][0][2];
-  const double y0o = P.vd[1][1][0], y1o = P.vd[1][1][1], y2o = P.vd[1][1][2];
-  const double z0i = P.vd[2][0][0], z1i = P.vd[2][0][1], z2i = P.vd[2][0][2];
-  const double z0o = P.vd[2][1][0], z1o = P.vd[2][1][1], z2o = P.vd[2][1][2];
   for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
-    const long long m0 = (long long)P.nx * row;
+    const long long m0 = (long long)nx * row;
     const RowExact q = row_exact(P, iy, iz);
+    double* const Rr = R + m0;
     if (iy == 0 || iz == 0 || iy == P.ny - 1 || iz == P.nz - 1) {
-      for (int ix = lane; ix < P.nx; ix += 32) R[m0 + ix] = row_outer(P, q, ix, E);
+      for (int ix = lane; ix < nx; ix += 32) Rr[ix] = row_outer(P, q, ix, E);
       continue;
     }
-    for (int ix0 = 0; ix0 < P.nx; ix0 += 32 * G) {
+    // the row's two face nodes, then its interior in groups of G x 32
+    if (lane < 2) {
+      const int ix = lane ? nx - 1 : 0;
+      Rr[ix] = row_outer(P, q, ix, E);
+    }
+    const double* const uc_r = un + m0;
+    const double* const uym_r = uc_r - sy;
+    const double* const uyp_r = uc_r + sy;
+    const double* const uzm_r = uc_r - sz;
+    const double* const uzp_r = uc_r + sz;
+    const uint8_t* const tg_r = P.tag + m0;
+    for (int ix0 = 1; ix0 < nx - 1; ix0 += 32 * G) {
       double uc[G], uym[G], uyp[G], uzm[G], uzp[G];
       int tg[G];
 #pragma unroll
       for (int g = 0; g < G; g++) {
         const int ix = ix0 + 32 * g + lane;
-        if (ix < P.nx) {
-          const long long m = m0 + ix;
-          tg[g] = P.tag[m];
-          uc[g] = un[m];
-          uym[g] = un[m - sy];
-          uyp[g] = un[m + sy];
-          uzm[g] = un[m - sz];
-          uzp[g] = un[m + sz];
+        if (ix < nx - 1) {
+          tg[g] = tg_r[ix];
+          uc[g] = uc_r[ix];
+          uym[g] = uym_r[ix];
+          uyp[g] = uyp_r[ix];
+          uzm[g] = uzm_r[ix];
+          uzp[g] = uzp_r[ix];
         }
       }
 #pragma unroll
       for (int g = 0; g < G; g++) {
         const int ix = ix0 + 32 * g + lane;
-        if (ix >= P.nx) break;
-        const long long m = m0 + ix;
-        double r;
-        if (ix == 0 || ix == P.nx - 1) {
-          r = row_outer(P, q, ix, E);
-        } else if (!(tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
-          const int side = tg[g] & TAG_OUT;
-          double sum = 0.0;
-          sum += uym[g] * (side ? y0o : y0i);
-          sum += uc[g] * (side ? y1o : y1i);
-          sum += uyp[g] * (side ? y2o : y2i);
-          const double ydt = dt * sum;
-          sum = 0.0;
-          sum += uzm[g] * (side ? z0o : z0i);
-          sum += uc[g] * (side ? z1o : z1i);
-          sum += uzp[g] * (side ? z2o : z2i);
-          const double zdt = dt * sum;
-          const double src = row_source(P, q, ix, E, side);
-          r = ydt + zdt;
-          r += uc[g];
-          r += dt * src;
-        } else {
-          continue;  // a MIB row: k_adi_rhs_mib writes it
-        }
-        R[m] = r;
+        if (ix >= nx - 1) break;
+        if (tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) continue;  // a MIB row: k_adi_rhs_mib writes it
+        const int side = tg[g] & TAG_OUT;
+        double sum = 0.0;
+        sum += uym[g] * P.vd[1][side][0];
+        sum += uc[g] * P.vd[1][side][1];
+        sum += uyp[g] * P.vd[1][side][2];
+        const double ydt = dt * sum;
+        sum = 0.0;
+        sum += uzm[g] * P.vd[2][side][0];
+        sum += uc[g] * P.vd[2][side][1];
+        sum += uzp[g] * P.vd[2][side][2];
+        const double zdt = dt * sum;
+        const double src = row_source(P, q, ix, E, side);
+        double r = ydt + zdt;
+        r += uc[g];
+        r += dt * src;
+        Rr[ix] = r;
       }
     }
   }
