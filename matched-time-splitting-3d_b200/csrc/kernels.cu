@@ -49,8 +49,8 @@ namespace {
       if (long long m = ix + (long long)(P).nx * row_; true)
 
 // RHS1 of a node that is a MIB row of some x, y or z block: the general form.
-__device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __restrict__ un, double E, long long m, int ix,
-                                           int iy, int iz, int tg) {
+__device__ __forceinline__ double adi_rhs_mib(const Dev& P, const double* __restrict__ un, double E, long long m,
+                                              int ix, int iy, int iz, int tg) {
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int side = tg & TAG_OUT;
   const double dt = P.dt;
@@ -166,12 +166,14 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
 }
 
 template <int G>
-__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un, double* __restrict__ R, double E) {
+__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                 double* __restrict__ R, double E) {
   k_adi_rhs_body<G>(P, blockIdx.x, gridDim.x, un, R, E);
 }
 
 // The MIB rows of RHS1, one thread per listed node.
-__device__ __forceinline__ void k_adi_rhs_mib_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ un, double* __restrict__ R, double E) {
+__device__ __forceinline__ void k_adi_rhs_mib_body(const Dev& P, unsigned cta_, unsigned ncta_,
+                                                   const double* __restrict__ un, double* __restrict__ R, double E) {
   const int k = cta_ * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   E = step_e(P, E, 2);
@@ -181,7 +183,8 @@ __device__ __forceinline__ void k_adi_rhs_mib_body(const Dev& P, unsigned cta_, 
   R[m] = adi_rhs_mib(P, un, E, m, ix, iy, iz, P.tag[m]);
 }
 
-__global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev P, const double* __restrict__ un, double* __restrict__ R, double E) {
+__global__ void __launch_bounds__(TPB) k_adi_rhs_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                     double* __restrict__ R, double E) {
   k_adi_rhs_mib_body(P, blockIdx.x, gridDim.x, un, R, E);
 }
 
@@ -208,7 +211,8 @@ __device__ __forceinline__ double ts_explicit_mib(const Dev& P, const double* __
 }
 
 template <int D>
-__device__ __forceinline__ void k_ts_explicit_mib_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ in, double* __restrict__ out) {
+__device__ __forceinline__ void k_ts_explicit_mib_body(const Dev& P, unsigned cta_, unsigned ncta_,
+                                                       const double* __restrict__ in, double* __restrict__ out) {
   const int k = cta_ * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   const long long m = P.mibnode[k];
@@ -220,12 +224,15 @@ __device__ __forceinline__ void k_ts_explicit_mib_body(const Dev& P, unsigned ct
 }
 
 template <int D>
-__global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__ Dev P, const double* __restrict__ in, double* __restrict__ out) {
+__global__ void __launch_bounds__(TPB) k_ts_explicit_mib(const __grid_constant__ Dev P,
+                                                         const double* __restrict__ in, double* __restrict__ out) {
   k_ts_explicit_mib_body<D>(P, blockIdx.x, gridDim.x, in, out);
 }
 
 template <int D>
-__device__ __forceinline__ void k_ts_explicit_body(const Dev& P, unsigned cta_, unsigned ncta_, const double* __restrict__ in, double* __restrict__ out, double eh) {
+__device__ __forceinline__ void k_ts_explicit_body(const Dev& P, unsigned cta_, unsigned ncta_,
+                                                   const double* __restrict__ in, double* __restrict__ out,
+                                                   double eh) {
   eh = step_e(P, eh, 1);
   const long long s = D == 0 ? 1 : (long long)P.nx;
   const int flag = D == 0 ? TAG_MIBX : TAG_MIBY;
@@ -281,7 +288,8 @@ __device__ __forceinline__ void k_ts_explicit_body(const Dev& P, unsigned cta_, 
 }
 
 template <int D>
-__global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in, double* __restrict__ out, double eh) {
+__global__ void __launch_bounds__(TPB) k_ts_explicit(const __grid_constant__ Dev P, const double* __restrict__ in,
+                                                     double* __restrict__ out, double eh) {
   k_ts_explicit_body<D>(P, blockIdx.x, gridDim.x, in, out, eh);
 }
 
@@ -333,7 +341,8 @@ __device__ __forceinline__ void load_head(const MibBlock* blk, const double* rbl
 // terms of D_xx_l lod.cc:960-1097, the Convert2Tri row operations) and stores
 // them for the sweep, which then spends no time on MIB data.
 template <int D, int KIND>
-__device__ __forceinline__ void k_block_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_, const SweepIO io, int nblk) {
+__device__ __forceinline__ void k_block_rhs_body(const Dev& P, unsigned cta_, unsigned ncta_, const SweepIO io,
+                                                 int nblk) {
   const int k = cta_ * TPB + threadIdx.x;
   if (k >= nblk) return;
   const MibBlock& b = P.blk[D][k];
@@ -1297,8 +1306,8 @@ __global__ void __launch_bounds__(TPB) kb_adi_rhs_mib(const Dev* __restrict__ Ps
 }
 
 template <int D>
-__global__ void __launch_bounds__(TPB) kb_ts_explicit(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items,
-                                                      int in) {
+__global__ void __launch_bounds__(TPB) kb_ts_explicit(const Dev* __restrict__ Ps,
+                                                      const BatchItem* __restrict__ items, int in) {
   BATCH_PROLOGUE
   k_ts_explicit_body<D>(P, w.cta, w.ncta, in ? P.u1 : P.u0, in ? P.u0 : P.u1, 0.0);
 }

@@ -18,7 +18,19 @@ import numpy as np
 from ._lib import (CROSSING_DTYPE, EXPORTS, METHODS, MtsError, check, lib_path, load, make_grid, make_params,
                    make_surface)
 
-__all__ = ["Spec", "Solver", "setup_host", "batch_advance", "batch_advance_steps", "MtsError", "CROSSING_DTYPE", "METHODS", "EXPORTS", "load", "lib_path"]
+__all__ = [
+    "Spec",
+    "Solver",
+    "setup_host",
+    "batch_advance",
+    "batch_advance_steps",
+    "MtsError",
+    "CROSSING_DTYPE",
+    "METHODS",
+    "EXPORTS",
+    "load",
+    "lib_path",
+]
 
 
 @dataclass

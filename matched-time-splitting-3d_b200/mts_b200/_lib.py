@@ -217,5 +217,5 @@ def make_surface(kind: str, params) -> mts_surface:
 
 
 def make_params(beta_in, beta_out, eq, method, mib, dt, t0=0.0) -> mts_params:
-    return mts_params(float(beta_in), float(beta_out), int(eq), METHODS[method] if isinstance(method, str) else int(method),
-                      int(mib), 0, float(dt), float(t0))
+    m = METHODS[method] if isinstance(method, str) else int(method)
+    return mts_params(float(beta_in), float(beta_out), int(eq), m, int(mib), 0, float(dt), float(t0))
