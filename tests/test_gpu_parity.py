@@ -187,3 +187,23 @@ def test_eq0_constant_solution_is_kept_at_257():
                   eq=0, method="adi", mib=2, dt=2.0 / 256)
     u, (lmax, l2, _), _ = run_gpu(spec, 3)
     assert lmax <= 1e-9 * 100.0, lmax
+
+
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+def test_gpu_without_crossings(method):
+    """An interface that crosses no grid line (a sphere between the nodes):
+    no MIB rows, no per-node factors, no jump data; GPU vs oracle, alone and
+    in a batch."""
+    spec = M.Spec(n=(17, 17, 17), surface="ellipsoid", surface_params=(1.0, 1.0, 1.0, 0.1, 0.0625, 0.0625, 0.0625),
+                  beta_in=1.0, beta_out=10.0, method=method, mib=2, dt=0.125)
+    tags, cr, _ = M.setup_host(spec)
+    assert len(cr) == 0
+    prob = O.Problem(n=spec.n, surface="ellipsoid", surface_params=spec.surface_params, beta_in=1.0, beta_out=10.0,
+                     method=method, mib=2, dt=0.125, steps=3)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    u, _, _ = run_gpu(spec, 3)
+    assert np.array_equal(u, u_or)
+    with M.Solver(spec) as s:
+        s.initialize()
+        M.batch_advance([s], 3)
+        assert np.array_equal(s.solution(), u_or)
