@@ -278,8 +278,9 @@ static int ctx_init(ctx* C, const mts_oracle_problem* p, const int8_t* tags,
   C->r = (double*)malloc(sizeof(double) * (size_t)nmax);
   C->ut = (double*)malloc(sizeof(double) * (size_t)nmax);
   C->jb = (double*)calloc((size_t)(ncr > 0 ? ncr : 1), sizeof(double));
-  if (cr) return build_lines(C, ncr);
-  return 0;
+  /* line tables are built even without crossings (ncr == 0, cr NULL): the
+     sweeps walk them for every line */
+  return build_lines(C, ncr);
 }
 
 static void ctx_free(ctx* C) {

@@ -80,3 +80,16 @@ def test_aux_bypass_is_solution_neutral():
             b = O.run_reference(prob, noaux=True)
             assert np.array_equal(a.u, b.u)
             assert a.crossings.tobytes() == b.crossings.tobytes()
+
+
+@needs_ref
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "lod-cn", "ts"])
+def test_oracle_without_crossings_matches_reference(method):
+    """A sphere between the grid nodes crosses no grid line: the oracle runs
+    with an empty crossing list and returns the reference's solution."""
+    prob = O.Problem(n=(17, 17, 17), surface_params=(1.0, 1.0, 1.0, 0.1, 0.0625, 0.0625, 0.0625), beta_in=1.0,
+                     beta_out=10.0, method=method, mib=2, dt=0.125, steps=3)
+    r = O.run_reference(prob, noaux=True)
+    assert len(r.crossings) == 0
+    u = O.port_run(prob, r.tags, r.crossings, r.u0)
+    assert np.array_equal(u, r.u)
