@@ -23,6 +23,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 REF_BIN = os.path.join(REF_DIR, "mts_ref")
 REF_BIN_NOAUX = os.path.join(REF_DIR, "mts_ref_noaux")
+# mts_ref_noaux with mts::GpuStepper (include/mts_reference_adapter.hpp)
+# linked in: --gpu runs the reference's time loop on libmts_b200.so
+REF_BIN_DROPIN = os.path.join(REF_DIR, "mts_dropin")
 PORT_LIB = os.path.join(REF_DIR, "libmts_oracle.so")
 
 METHODS = {"adi": 0, "lod-ie": 1, "lod-cn": 2, "ts": 3}
@@ -83,19 +86,26 @@ class RefResult:
     crossings: np.ndarray = field(repr=False)
 
 
-def reference_available(noaux: bool = False) -> bool:
-    return os.path.exists(REF_BIN_NOAUX if noaux else REF_BIN)
+def reference_available(noaux: bool = False, dropin: bool = False) -> bool:
+    return os.path.exists(REF_BIN_DROPIN if dropin else REF_BIN_NOAUX if noaux else REF_BIN)
 
 
-def run_reference(prob: Problem, noaux: bool = False, timeout: float = 3600) -> RefResult:
+def run_reference(prob: Problem, noaux: bool = False, timeout: float = 3600, dropin_gpu: bool = False,
+                  binary: str | None = None) -> RefResult:
     """Run the reference binary on ``prob``; raises RuntimeError when the
     reference aborts (it exits 0 on setup failures, so the JSON line is the
-    success signal, as src/mesh/mesh.cc:64-65 and intersection.cc:2827 show)."""
-    binary = REF_BIN_NOAUX if noaux else REF_BIN
+    success signal, as src/mesh/mesh.cc:64-65 and intersection.cc:2827 show).
+
+    dropin_gpu: run the reference's setup and time loop with mts::GpuStepper
+    stepping on the GPU in place of Douglas_ADI / LOD / TS (mts_dropin --gpu);
+    the setup is the noaux one.  binary: run this build instead."""
+    binary = binary or (REF_BIN_DROPIN if dropin_gpu else REF_BIN_NOAUX if noaux else REF_BIN)
     with tempfile.TemporaryDirectory() as td:
         fu, fu0 = os.path.join(td, "u.bin"), os.path.join(td, "u0.bin")
         ft, fm = os.path.join(td, "tags.bin"), os.path.join(td, "mib.bin")
         cmd = [binary, *prob.ref_args(), "--dump-u", fu, "--dump-u0", fu0, "--dump-tags", ft, "--dump-mib", fm]
+        if dropin_gpu:
+            cmd.append("--gpu")
         cp = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         lines = [ln for ln in cp.stdout.splitlines() if ln.startswith("{")]
         if cp.returncode != 0 or not lines:

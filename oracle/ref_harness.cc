@@ -37,6 +37,9 @@
 #include "temporal/douglas_adi.h"
 #include "temporal/lod.h"
 #include "temporal/trapezoidal.h"
+#ifdef MTS_DROPIN
+#include "mts_reference_adapter.hpp"
+#endif
 
 using namespace std;
 
@@ -162,6 +165,7 @@ struct Args {
   int steps = -1;
   double t_end = 1.0;
   string dump_u, dump_tags, dump_mib, dump_u0;
+  bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
 };
 
 [[noreturn]] void usage() {
@@ -170,7 +174,11 @@ struct Args {
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
           "        --beta bi bo --eq 0|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
-          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F]\n");
+          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F]\n"
+#ifdef MTS_DROPIN
+          "        [--gpu]\n"
+#endif
+  );
   exit(2);
 }
 
@@ -229,6 +237,10 @@ Args parse(int argc, char** argv) {
     } else if (k == "--dump-mib") {
       need(1);
       a.dump_mib = argv[++i];
+#ifdef MTS_DROPIN
+    } else if (k == "--gpu") {
+      a.gpu = true;
+#endif
     } else {
       usage();
     }
@@ -390,44 +402,59 @@ int main(int argc, char** argv) {
     l2 = sqrt(l2 / (1.0 * nx * ny * nz));
   };
 
+  // The reference's time loops (src/helper.h:199-426): Initialization at t0,
+  // then one Solve_2nd per step with the exact solutions at the step's
+  // times.  St is the reference's stepper or, with --gpu, mts::GpuStepper in
+  // its place: the loop is the same code for both.
+  auto run = [&](auto& st, auto&& solve) {
+    st.Initialization(*make_eq(a, a.t0, beta), uh);
+    if (!a.dump_u0.empty()) dump_field(a.dump_u0, uh, nx, ny, nz);
+    auto s0 = chrono::steady_clock::now();
+    for (int j = 0; j < steps; j++) {
+      t_now += a.dt;
+      solve(st);
+    }
+    step_seconds = chrono::duration<double>(chrono::steady_clock::now() - s0).count();
+  };
+  auto adi_step = [&](auto& st) {
+    auto eq = make_eq(a, t_now, beta);
+    st.Solve_2nd(*eq, inter, uh, beta);
+  };
+  char lod_m = a.method == "lod-ie" ? 'I' : 'C';
+  auto lod_step = [&](auto& st) {
+    auto eq = make_eq(a, t_now, beta);
+    st.Solve_2nd(*eq, inter, uh, beta, lod_m);
+  };
+  auto ts_step = [&](auto& st) {
+    auto e0 = make_eq(a, t_now - a.dt, beta);
+    auto eh = make_eq(a, t_now - 0.5 * a.dt, beta);
+    auto e1 = make_eq(a, t_now, beta);
+    st.Solve_2nd(*e0, *eh, *e1, inter, uh, beta);
+  };
+
+  bool lod = a.method == "lod-ie" || a.method == "lod-cn";
+  if (a.method != "adi" && !lod && a.method != "ts") usage();
+#ifdef MTS_DROPIN
+  if (a.gpu) {
+    int method = a.method == "adi" ? MTS_ADI : a.method == "lod-ie" ? MTS_LOD_IE : a.method == "lod-cn" ? MTS_LOD_CN : MTS_TS;
+    mts::GpuStepper st(inter, mesh, beta, time, 2, method, a.eq);
+    if (a.method == "adi")
+      run(st, adi_step);
+    else if (lod)
+      run(st, lod_step);
+    else
+      run(st, ts_step);
+  } else
+#endif
   if (a.method == "adi") {
-    Douglas_ADI adi(inter, mesh, beta, time, 2);
-    adi.Initialization(*make_eq(a, a.t0, beta), uh);
-    if (!a.dump_u0.empty()) dump_field(a.dump_u0, uh, nx, ny, nz);
-    auto s0 = chrono::steady_clock::now();
-    for (int j = 0; j < steps; j++) {
-      t_now += a.dt;
-      auto eq = make_eq(a, t_now, beta);
-      adi.Solve_2nd(*eq, inter, uh, beta);
-    }
-    step_seconds = chrono::duration<double>(chrono::steady_clock::now() - s0).count();
-  } else if (a.method == "lod-ie" || a.method == "lod-cn") {
-    char m = a.method == "lod-ie" ? 'I' : 'C';
-    LOD lod(inter, mesh, beta, time);
-    lod.Initialization(*make_eq(a, a.t0, beta), uh);
-    if (!a.dump_u0.empty()) dump_field(a.dump_u0, uh, nx, ny, nz);
-    auto s0 = chrono::steady_clock::now();
-    for (int j = 0; j < steps; j++) {
-      t_now += a.dt;
-      auto eq = make_eq(a, t_now, beta);
-      lod.Solve_2nd(*eq, inter, uh, beta, m);
-    }
-    step_seconds = chrono::duration<double>(chrono::steady_clock::now() - s0).count();
-  } else if (a.method == "ts") {
-    TS ts(inter, mesh, beta, time);
-    ts.Initialization(*make_eq(a, a.t0, beta), uh);
-    if (!a.dump_u0.empty()) dump_field(a.dump_u0, uh, nx, ny, nz);
-    auto s0 = chrono::steady_clock::now();
-    for (int j = 0; j < steps; j++) {
-      t_now += a.dt;
-      auto e0 = make_eq(a, t_now - a.dt, beta);
-      auto eh = make_eq(a, t_now - 0.5 * a.dt, beta);
-      auto e1 = make_eq(a, t_now, beta);
-      ts.Solve_2nd(*e0, *eh, *e1, inter, uh, beta);
-    }
-    step_seconds = chrono::duration<double>(chrono::steady_clock::now() - s0).count();
+    Douglas_ADI st(inter, mesh, beta, time, 2);
+    run(st, adi_step);
+  } else if (lod) {
+    LOD st(inter, mesh, beta, time);
+    run(st, lod_step);
   } else {
-    usage();
+    TS st(inter, mesh, beta, time);
+    run(st, ts_step);
   }
   norms(*make_eq(a, t_now, beta));
   if (!a.dump_u.empty()) dump_field(a.dump_u, uh, nx, ny, nz);

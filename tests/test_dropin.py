@@ -1,0 +1,70 @@
+"""The drop-in: the reference's own setup and time loop, with
+mts::GpuStepper (include/mts_reference_adapter.hpp) constructed and called
+where the loop constructs and calls Douglas_ADI, LOD or TS.
+
+oracle/_ref/mts_dropin is the noaux reference build with the harness compiled
+-DMTS_DROPIN and linked against libmts_b200.so; `--gpu` selects the adapter.
+Its initial field, final field and error norms must equal the reference
+stepper's bit for bit."""
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+needs_dropin = pytest.mark.skipif(not O.reference_available(dropin=True),
+                                  reason="drop-in build (oracle/_ref/mts_dropin) absent")
+
+CASES = [
+    # (id, Problem)
+    ("ts_l2_ellipsoid_17", O.Problem(n=(17, 17, 17), surface="ellipsoid",
+                                     surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
+                                     beta_in=1.0, beta_out=1000.0, method="ts", mib=2, dt=0.125, steps=3)),
+    ("adi_l1_torus_25", O.Problem(n=(25, 25, 25), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0,
+                                  beta_out=10.0, method="adi", mib=1, dt=2.0 / 24, steps=4)),
+    ("lodcn_l2_sphere_33", O.Problem(n=(33, 33, 33), beta_in=1.0, beta_out=10.0, method="lod-cn", mib=2,
+                                     dt=1.0 / 32, steps=4)),
+    ("lodie_l1_eq0_anisotropic", O.Problem(n=(21, 19, 23), surface="ellipsoid",
+                                           surface_params=(0.55, 0.6, 0.45, 1.0, -0.04, 0.03, 0.01), beta_in=1.0,
+                                           beta_out=0.01, eq=0, method="lod-ie", mib=1, dt=0.1, steps=3)),
+    # the reference's shipped configuration: ADI + MIB-L1, r = 0.49 sphere,
+    # beta 1/10, dt = h/2, to t = 1
+    ("config0_adi_l1_sphere_33", O.Problem(n=(33, 33, 33), beta_in=1.0, beta_out=10.0, method="adi", mib=1,
+                                           dt=1.0 / 32, steps=32)),
+]
+
+
+@needs_dropin
+def test_dropin_without_gpu_flag_is_the_reference():
+    """Without --gpu the drop-in binary runs the reference stepper (the loop
+    code is shared), bit for bit the noaux reference."""
+    prob = CASES[0][1]
+    a = O.run_reference(prob, noaux=True)
+    b = O.run_reference(prob, binary=O.REF_BIN_DROPIN)
+    assert np.array_equal(a.u0, b.u0) and np.array_equal(a.u, b.u)
+    assert a.info["lmax"] == b.info["lmax"] and a.info["l2"] == b.info["l2"]
+
+
+@needs_dropin
+def test_dropin_fails_loudly_without_a_device():
+    """--gpu never falls back to the CPU: with no CUDA device visible the
+    adapter throws and the process exits non-zero without a result line."""
+    cmd = [O.REF_BIN_DROPIN, *CASES[0][1].ref_args(), "--gpu"]
+    cp = subprocess.run(cmd, capture_output=True, text=True, timeout=120, env={"CUDA_VISIBLE_DEVICES": ""})
+    assert cp.returncode != 0
+    assert not [ln for ln in cp.stdout.splitlines() if ln.startswith("{")]
+    assert "mts:" in cp.stderr
+
+
+@pytest.mark.gpu
+@needs_dropin
+@pytest.mark.parametrize("name,prob", CASES, ids=[c[0] for c in CASES])
+def test_dropin_gpu_equals_reference_bitwise(name, prob):
+    ref = O.run_reference(prob, noaux=True)
+    gpu = O.run_reference(prob, dropin_gpu=True)
+    assert np.array_equal(gpu.u0, ref.u0), name
+    diff = np.max(np.abs(gpu.u - ref.u))
+    assert np.array_equal(gpu.u, ref.u), f"{name}: max |gpu - reference| = {diff}"
+    for k in ("t", "lmax", "l2", "argmax", "ncross"):
+        assert gpu.info[k] == ref.info[k], (name, k, gpu.info[k], ref.info[k])
