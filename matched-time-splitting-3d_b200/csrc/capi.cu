@@ -1142,8 +1142,27 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
     return fail(MTS_ERR_ARG, "precision must be MTS_PRECISION_PLAIN or MTS_PRECISION_MIXED");
   if (precision == MTS_PRECISION_MIXED) {
     if (h->prm.method != MTS_ADI) return fail(MTS_ERR_ARG, "the mixed-precision form is built for Douglas-ADI only");
-    if (!mts::mixed_shape_fits(std::max(h->g.nx, std::max(h->g.ny, h->g.nz))))
+    const int nmax = std::max(h->g.nx, std::max(h->g.ny, h->g.nz));
+    if (!mts::mixed_shape_fits(nmax))
       return fail(MTS_ERR_ARG, "grid lines too long for the mixed-precision sweeps' shared memory");
+    if (mts::mixed_segments_fit(nmax) && !h->dev.cib[0]) {
+      // the segmented solves' per-node coefficients, once per handle
+      const size_t N = (size_t)h->g.nodes();
+      const int nd[3] = {h->g.nx, h->g.ny, h->g.nz};
+      for (int d = 0; d < 3; d++) {
+        float *ib = nullptr, *p = nullptr, *q = nullptr, *tab = nullptr;
+        CUDA_TRY(h->put(&ib, (const float*)nullptr, N));
+        CUDA_TRY(h->put(&p, (const float*)nullptr, N));
+        CUDA_TRY(h->put(&q, (const float*)nullptr, N));
+        CUDA_TRY(h->put(&tab, (const float*)nullptr, (size_t)6 * nd[d]));
+        h->dev.cib[d] = ib;
+        h->dev.cp[d] = p;
+        h->dev.cq[d] = q;
+        h->dev.ctab[d] = tab;
+      }
+      mts::build_mixed_coefs(h->dev, h->stream);
+      CUDA_TRY(cudaGetLastError());
+    }
   }
   h->dev.precision = precision;
   return MTS_OK;

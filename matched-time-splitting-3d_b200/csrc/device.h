@@ -108,6 +108,18 @@ struct Dev {
   const float* fib32[3];      // per node 1/bet of crossing lines from L1
   const float* fgam32[3];
   float* rblk32[3];           // block rows' right-hand sides after Convert2Tri
+  // Dense per-node coefficients of the segmented FP32 solves, built on the
+  // device when the mixed form is switched on (null before, and for grids
+  // whose lines are too long for them): for row j of a direction-d line,
+  //   cib = 1/bet_j,  cp = -a_j/bet_j (forward multiplier, 0 on face rows),
+  //   cq = -gam_{j+1} (backward multiplier, 0 on the last row).
+  // They are filled only for lines that cross the interface; every other
+  // interior line takes its row's values from ctab[d][side][{ib, p, q}][row]
+  // by the side of its row 1.
+  float* cib[3];
+  float* cp[3];
+  float* cq[3];
+  float* ctab[3];
   int precision;              // 0 plain FP64, 1 mixed
   // Replayable steps (batches captured in a CUDA graph): when tsched is set,
   // kernels take the step's exp(-t) factors from tsched[3*(*tstep) + {0: t_prev,
@@ -145,6 +157,9 @@ int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t 
 void configure_mixed_kernels();
 int mixed_sweep_threads();            // threads per CTA of the FP32 sweeps
 bool mixed_shape_fits(int nmax);      // their shared memory within the limit
+bool mixed_segments_fit(int n);       // the segmented solves take lines of n rows (else the ring sweeps run)
+// Fills Dev::cib/cp/cq (allocated by the caller) from the FP64 factors.
+int build_mixed_coefs(const Dev& P, cudaStream_t stream);
 // Batched plain steps (kernels.cu): problems of one method advance together,
 // one launch per kernel of the step for all of them.  A launch's CTAs are
 // listed as items (problem, the CTA's index in that problem's own grid, the

@@ -82,8 +82,9 @@ template <int D>
 __device__ __forceinline__ void decode_line(const Dev& P, long long t, Line& L) {
   int n1 = D == 0 ? P.ny : P.nx;
   int n2 = D == 2 ? P.ny : P.nz;
-  L.i1 = (int)(t % n1);
-  L.i2 = (int)(t / n1);
+  // a direction has n1*n2 < 2^31 lines: 32-bit division
+  L.i1 = (int)t % n1;
+  L.i2 = (int)t / n1;
   L.lid = L.i1 * n2 + L.i2;
   if (D == 0) {
     L.base = (long long)P.nx * (L.i1 + (long long)P.ny * L.i2);
@@ -291,6 +292,10 @@ __device__ __forceinline__ double row_source(const Dev& P, const RowExact& q, in
 template <bool B>
 struct BoolC {
   static constexpr bool value = B;
+};
+template <int I>
+struct IntC {
+  static constexpr int value = I;
 };
 
 }  // namespace

@@ -1,19 +1,18 @@
 // Time-stepping kernels for sm_100a.
 //
 // Implicit line sweeps (the Thomas solves, douglas_adi.cc:1784-1807 and the
-// LOD/TS copies) run as one persistent CTA of 128 threads per SM; each thread
-// solves one grid line at a time, lines of a warp being consecutive in the
-// fast index.  Per line:
-//   * forward: the inputs of the line are staged into a 4-chunk shared-memory
-//     ring with cp.async, 2-3 chunks (32-48 rows) ahead of use; the
-//     right-hand side of chunk k+1 is built from the ring (3-point stencil,
-//     MIB fictitious-point rows, source terms) while chunk k runs the
-//     elimination recurrence; the MIB row blocks of chunk k are mixed in
-//     (Convert2Tri row operations replayed on the right-hand side) just
-//     before their rows are eliminated;
-//   * the factors c_{j-1}/bet and partial solutions d'_j go to per-thread
-//     scratch laid out [row][thread] (coalesced in every direction, reused
-//     line after line, so it lives in L2);
+// LOD/TS copies) run as one persistent CTA of 128-512 threads per SM (the
+// sweep shape); each thread solves one grid line at a time, lines of a warp
+// being consecutive in the fast index.  The Thomas factors (bet, gam) are
+// computed once at setup.  Per line:
+//   * forward: the inputs of the line (and its per-node factors from its
+//     first MIB row on) are staged into a shared-memory ring with cp.async,
+//     chunks ahead of use; each row's right-hand side is built from the ring
+//     (3-point stencil, source terms), the MIB row blocks' right-hand sides
+//     come from the block pre-pass (Convert2Tri row operations replayed on
+//     them), and the elimination recurrence runs over the chunk;
+//   * the partial solutions d'_j go to per-thread scratch laid out
+//     [row][thread] (coalesced in every direction, reused line after line);
 //   * backward: the scratch is staged back through the same ring and the
 //     solution is written once.
 // The inside/outside side of a node, which selects the stencil weights and
@@ -104,6 +103,11 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
   const int nx = P.nx, nrows = P.ny * P.nz;
   const long long sy = nx, sz = (long long)nx * P.ny;
   const double dt = P.dt;
+  // the y and z stencil weights of both sides in registers: a node's side
+  // selects one of two specialised bodies (uniform over a warp away from the
+  // interface) instead of indexing the weights per node
+  const double wy[2][3] = {{P.vd[1][0][0], P.vd[1][0][1], P.vd[1][0][2]}, {P.vd[1][1][0], P.vd[1][1][1], P.vd[1][1][2]}};
+  const double wz[2][3] = {{P.vd[2][0][0], P.vd[2][0][1], P.vd[2][0][2]}, {P.vd[2][1][0], P.vd[2][1][1], P.vd[2][1][2]}};
   for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)nx * row;
@@ -144,22 +148,25 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
         const int ix = ix0 + 32 * g + lane;
         if (ix >= nx - 1) break;
         if (tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) continue;  // a MIB row: k_adi_rhs_mib writes it
-        const int side = tg[g] & TAG_OUT;
-        double sum = 0.0;
-        sum += uym[g] * P.vd[1][side][0];
-        sum += uc[g] * P.vd[1][side][1];
-        sum += uyp[g] * P.vd[1][side][2];
-        const double ydt = dt * sum;
-        sum = 0.0;
-        sum += uzm[g] * P.vd[2][side][0];
-        sum += uc[g] * P.vd[2][side][1];
-        sum += uzp[g] * P.vd[2][side][2];
-        const double zdt = dt * sum;
-        const double src = row_source(P, q, ix, E, side);
-        double r = ydt + zdt;
-        r += uc[g];
-        r += dt * src;
-        Rr[ix] = r;
+        auto node = [&](auto S) {
+          constexpr int sd = decltype(S)::value;
+          double sum = 0.0;
+          sum += uym[g] * wy[sd][0];
+          sum += uc[g] * wy[sd][1];
+          sum += uyp[g] * wy[sd][2];
+          const double ydt = dt * sum;
+          sum = 0.0;
+          sum += uzm[g] * wz[sd][0];
+          sum += uc[g] * wz[sd][1];
+          sum += uzp[g] * wz[sd][2];
+          const double zdt = dt * sum;
+          const double src = row_source(P, q, ix, E, sd);
+          double r = ydt + zdt;
+          r += uc[g];
+          r += dt * src;
+          return r;
+        };
+        Rr[ix] = (tg[g] & TAG_OUT) ? node(IntC<1>{}) : node(IntC<0>{});
       }
     }
   }

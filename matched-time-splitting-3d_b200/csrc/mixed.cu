@@ -17,6 +17,8 @@
 // increment of one step, never the accumulated solution.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device.h"
 #include "device_common.cuh"
 
@@ -34,12 +36,15 @@ __global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P
   const int lane = threadIdx.x & 31;
   const int nrows = P.ny * P.nz;
   const double dt = P.dt;
-  const double x0i = P.vd[0][0][0], x1i = P.vd[0][0][1], x2i = P.vd[0][0][2];
-  const double x0o = P.vd[0][1][0], x1o = P.vd[0][1][1], x2o = P.vd[0][1][2];
-  const double y0i = P.vd[1][0][0], y1i = P.vd[1][0][1], y2i = P.vd[1][0][2];
-  const double y0o = P.vd[1][1][0], y1o = P.vd[1][1][1], y2o = P.vd[1][1][2];
-  const double z0i = P.vd[2][0][0], z1i = P.vd[2][0][1], z2i = P.vd[2][0][2];
-  const double z0o = P.vd[2][1][0], z1o = P.vd[2][1][1], z2o = P.vd[2][1][2];
+  // stencil weights [dir][side][k] in registers; a node's side selects one
+  // of two specialised bodies (uniform over a warp away from the interface)
+  double wv[3][2][3];
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int sd = 0; sd < 2; sd++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) wv[d][sd][k] = P.vd[d][sd][k];
   for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)P.nx * row;
@@ -76,11 +81,14 @@ __global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P
         if (ix == 0 || ix == P.nx - 1) {
           r = row_outer(P, q, ix, E) - uc[g];
         } else if (!(tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
-          const int side = tg[g] & TAG_OUT;
-          const double sx = (uxm[g] * (side ? x0o : x0i) + uc[g] * (side ? x1o : x1i)) + uxp[g] * (side ? x2o : x2i);
-          const double sy_ = (uym[g] * (side ? y0o : y0i) + uc[g] * (side ? y1o : y1i)) + uyp[g] * (side ? y2o : y2i);
-          const double sz_ = (uzm[g] * (side ? z0o : z0i) + uc[g] * (side ? z1o : z1i)) + uzp[g] * (side ? z2o : z2i);
-          r = dt * (((sx + sy_) + sz_) + row_source(P, q, ix, E, side));
+          auto node = [&](auto S) {
+            constexpr int sd = decltype(S)::value;
+            const double sx = (uxm[g] * wv[0][sd][0] + uc[g] * wv[0][sd][1]) + uxp[g] * wv[0][sd][2];
+            const double sy_ = (uym[g] * wv[1][sd][0] + uc[g] * wv[1][sd][1]) + uyp[g] * wv[1][sd][2];
+            const double sz_ = (uzm[g] * wv[2][sd][0] + uc[g] * wv[2][sd][1]) + uzp[g] * wv[2][sd][2];
+            return dt * (((sx + sy_) + sz_) + row_source(P, q, ix, E, sd));
+          };
+          r = (tg[g] & TAG_OUT) ? node(IntC<1>{}) : node(IntC<0>{});
         } else {
           continue;  // a MIB row: k_adi_resid_mib writes it
         }
@@ -142,8 +150,10 @@ __global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ D
 
 // Block pre-pass: the Convert2Tri row operations (douglas_adi.cc:1554-1675)
 // on the right-hand sides of each block's rows, in FP64, stored in FP32.
-template <int D>
-__global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev P, const float* __restrict__ f,
+// INPLACE (the segmented solves): the results replace the rows' right-hand
+// sides in the field, else they go to rblk32 for the ring sweeps.
+template <int D, bool INPLACE>
+__global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev P, float* __restrict__ f,
                                                      int nblk) {
   const int k = blockIdx.x * TPB + threadIdx.x;
   if (k >= nblk) return;
@@ -164,7 +174,10 @@ __global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev
     r[2] -= b.rate[4] * r[1];
     r[0] -= b.rate[5] * r[1];
   }
-  for (int q = 0; q < 3; q++) P.rblk32[D][3 * k + q] = (float)r[q];
+  if (INPLACE)
+    for (int q = 0; q < b.kind; q++) f[L.base + (long long)(b.L + q) * L.s] = (float)r[q];
+  else
+    for (int q = 0; q < 3; q++) P.rblk32[D][3 * k + q] = (float)r[q];
 }
 
 struct BlockHead32 {
@@ -460,17 +473,291 @@ __global__ void __launch_bounds__(NT, 1) k_sweep32(const __grid_constant__ Dev P
 #undef RC
 }
 
-// Shape of the FP32 sweeps (rows per chunk, ring chunks, threads per CTA):
-// 448 threads on each of the 148 SMs cover the 66,049 lines of a 257^3 grid
-// in one wave.
-constexpr int S32_CH = 8, S32_NS = 4, S32_NT = 448;
+// ---------------------------------------------------------------------------
+// Segmented FP32 line solves.  With the factors fixed, both Thomas
+// recurrences are first-order and linear:
+//   forward   d_j = (r_j - a_j d_{j-1}) / bet_j = r_j ib_j + p_j d_{j-1}
+//   backward  x_j = d_j - gam_{j+1} x_{j+1}    = d_j + q_j x_{j+1}
+// with ib_j = 1/bet_j, p_j = -a_j/bet_j and q_j = -gam_{j+1} stored per node
+// (Dev::cib/cp/cq; block rows carry their Convert2Tri sub-diagonal, face
+// rows p = 0, the last row q = 0).  A line is cut into segments that run at
+// once: each runs the recurrence from a zero carry while it multiplies up
+// its multipliers (P_j, Q_j); the segments' end states (value, product)
+// compose into the carry of every segment, and the true values are
+//   d_j = d~_j + P_j C,   x_j = x~_j + Q_j X.
+// The rounding differs from one sequential pass only within the FP32
+// increment.  The block pre-pass writes the block rows' right-hand sides into
+// the field in place first, so every row reads its right-hand side there.
 
+// Coefficients of one direction, one thread per line that crosses the
+// interface, walking the line as the sequential sweep does (side of the
+// regular rows from the line's start and after each block, factors from the
+// prefix tables up to the first MIB row and per node from there on).
 template <int D>
-void sweep32(const Dev& P, float* f, cudaStream_t st) {
-  if (P.nblk[D] > 0) k_block_rhs32<D><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
-  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
-  k_sweep32<D, S32_CH, S32_NS, S32_NT>
-      <<<sweep_grid(P, nlines<D>(P), S32_NT), S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f);
+__global__ void __launch_bounds__(TPB) k_coef32(const __grid_constant__ Dev P) {
+  const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (t >= nlines<D>(P)) return;
+  Line L;
+  decode_line<D>(P, t, L);
+  if (L.boundary) return;
+  const int bfirst = P.bstart[D][L.lid], bend = P.bstart[D][L.lid + 1];
+  if (bfirst == bend) return;  // no crossing: the line reads the row tables
+  const int n = L.n;
+  const long long s = L.s;
+  const int ls = P.lside[D][L.lid];
+  const MibBlock* const blk = P.blk[D];
+  const int L1 = blk[bfirst].L;
+  const double* const pt = P.ptab[D][(ls >> 1) & 1];
+  int b = bfirst;
+  int side = (ls >> 1) & 1;
+  for (int j = 0; j < n; j++) {
+    const long long g = L.base + (long long)j * s;
+    const double bet = j >= L1 ? P.fbet[D][g] : pt[2 * j];
+    double a;
+    if (j == 0 || j == n - 1) {
+      a = 0.0;
+    } else if (b < bend && j >= blk[b].L) {
+      const int q = j - blk[b].L;
+      a = blk[b].ia[q];
+      if (q == blk[b].kind - 1) {
+        side = (blk[b].sides >> q) & 1;
+        b++;
+      }
+    } else {
+      a = P.ia[D][side];
+    }
+    const double gn = j == n - 1 ? 0.0 : j + 1 >= L1 ? P.fgam[D][g + s] : pt[2 * (j + 1) + 1];
+    P.cib[D][g] = (float)(1.0 / bet);
+    P.cp[D][g] = (float)(-(a / bet));
+    P.cq[D][g] = (float)(-gn);
+  }
+}
+
+// Row tables of the lines without crossings: [side][ib, p, q][row], from the
+// prefix tables of that side.
+template <int D>
+__global__ void __launch_bounds__(TPB) k_ctab32(const __grid_constant__ Dev P) {
+  const int n = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  const int i = blockIdx.x * TPB + threadIdx.x;
+  if (i >= 2 * n) return;
+  const int side = i / n, j = i % n;
+  const double* const pt = P.ptab[D][side];
+  const double bet = pt[2 * j];
+  const double a = j == 0 || j == n - 1 ? 0.0 : P.ia[D][side];
+  const double gn = j == n - 1 ? 0.0 : pt[2 * (j + 1) + 1];
+  float* const T = P.ctab[D] + (size_t)side * 3 * n;
+  T[j] = (float)(1.0 / bet);
+  T[n + j] = (float)(-(a / bet));
+  T[2 * n + j] = (float)(-gn);
+}
+
+// One warp per line, every direction.  A line's rows (right-hand side, and
+// for a crossing line its 1/bet, p, q) are copied into the warp's
+// shared-memory rows; lane l runs rows [l MX, l MX + MX) (MX odd: the lanes'
+// stride falls on distinct banks); the segment carries are warp scans
+// (shuffles) of the affine end maps; the solution goes back out through the
+// same rows.  x lines are contiguous, so a warp copies its own line.  y and
+// z lines are strided, so the CTA copies its 8 lines together, 8 neighbours
+// (32 bytes) per row at a time.
+// ACC (z): the increment is added to the FP64 state instead of being stored,
+// face lines included, so that u^{n+1} = u^n + d at every node.
+constexpr int WL_WARPS = 8;
+
+template <int MX>
+constexpr size_t wline_smem() {
+  // row tables 2 x 3 x R, then per warp r, ib, p, q (R each) + 4 floats of bank padding
+  return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)WL_WARPS * (4 * 32 * MX + 4));
+}
+
+template <int D, int MX, bool ACC>
+__global__ void __launch_bounds__(32 * WL_WARPS) k_wline32(const __grid_constant__ Dev P, float* __restrict__ f,
+                                                         double* __restrict__ u) {
+  static_assert(MX & 1, "odd rows per lane");
+  static_assert(!ACC || D == 2, "the increment is accumulated after the z solve");
+  constexpr int R = 32 * MX;
+  constexpr int LS = 4 * R + 4;  // a warp's rows: 4 fields of R, and padding so that the
+                                 // 8 lines of a cooperative copy fall on distinct banks
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ float sw[];
+  const int n = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  float* const tab = sw;  // [side][ib, p, q][R]
+  float* const buf = sw + 6 * R;
+  for (int i = threadIdx.x; i < 6 * n; i += 32 * WL_WARPS) tab[(i / n) * R + i % n] = P.ctab[D][i];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  float* const sr = buf + w * LS;
+  const long long nl = nlines<D>(P);
+  const float* __restrict__ cib = P.cib[D];
+  const float* __restrict__ cpp = P.cp[D];
+  const float* __restrict__ cqq = P.cq[D];
+  const int jb = l * MX;
+  // y, z: this thread's share of the cooperative copies, line c of the 8
+  const int c = threadIdx.x & 7, jc = threadIdx.x >> 3;
+  float* const cr = buf + c * LS;
+
+  for (long long t0 = (long long)blockIdx.x * WL_WARPS; t0 < nl; t0 += (long long)gridDim.x * WL_WARPS) {
+    const long long t = t0 + w;
+    const bool act = t < nl;
+    Line L;
+    decode_line<D>(P, act ? t : nl - 1, L);
+    const bool solve = act && !L.boundary;  // uniform over the warp
+    bool cross = false;
+    int side0 = 0;
+    if (solve) {
+      cross = P.bstart[D][L.lid + 1] > P.bstart[D][L.lid];
+      side0 = (P.lside[D][L.lid] >> 1) & 1;
+    }
+
+    // ---- copy in
+    Line Lc;
+    bool stc = false;
+    if (D == 0) {
+      __syncwarp();  // the previous line's stores have read the rows
+      if (solve) {
+#pragma unroll
+        for (int k = 0; k < MX; k++) {
+          const int j = l + 32 * k;
+          if (j < n) {
+            const long long g = L.base + j;
+            cp_async4(sr + j, f + g);
+            if (cross) {
+              cp_async4(sr + R + j, cib + g);
+              cp_async4(sr + 2 * R + j, cpp + g);
+              cp_async4(sr + 3 * R + j, cqq + g);
+            }
+          }
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncwarp();
+    } else {
+      const long long tc = t0 + c;
+      const bool actc = tc < nl;
+      decode_line<D>(P, actc ? tc : nl - 1, Lc);
+      const bool solvec = actc && !Lc.boundary;
+      stc = solvec || (ACC && actc);  // (ACC) face lines pass their right-hand side through
+      const bool crossc = solvec && P.bstart[D][Lc.lid + 1] > P.bstart[D][Lc.lid];
+      __syncthreads();  // the previous lines' stores have read the rows
+      if (stc) {
+        const long long s32 = 32 * Lc.s;
+        const float* gf = f + Lc.base + (long long)jc * Lc.s;
+#pragma unroll
+        for (int m = 0; m < MX; m++) {
+          const int j = jc + 32 * m;
+          if (j < n) {
+            const long long o = m * s32;
+            cp_async4(cr + j, gf + o);
+            if (crossc) {
+              const long long g = (gf - f) + o;
+              cp_async4(cr + R + j, cib + g);
+              cp_async4(cr + 2 * R + j, cpp + g);
+              cp_async4(cr + 3 * R + j, cqq + g);
+            }
+          }
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+    }
+
+    // ---- solve this warp's line
+    if (solve) {
+      const float* const si = cross ? sr + R : tab + side0 * 3 * R;
+      const float* const sp = si + R;
+      const float* const sq = sp + R;
+      float d[MX], pm[MX];
+      float dl = 0.0f, pl = 1.0f;
+#pragma unroll
+      for (int k = 0; k < MX; k++) {
+        const int j = jb + k;
+        if (j < n) {
+          const float p = sp[j];
+          dl = __fmaf_rn(p, dl, __fmul_rn(sr[j], si[j]));
+          pl = __fmul_rn(pl, p);
+          d[k] = dl;
+          pm[k] = pl;
+        }
+      }
+      // inclusive scan of the maps c -> pl c + dl over the lanes; the carry
+      // into lane l is the composition over lanes < l applied to 0 (lane 0
+      // starts at face row 0, whose p = 0)
+      float A = pl, B = dl;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const float Ap = __shfl_up_sync(FULL, A, off), Bp = __shfl_up_sync(FULL, B, off);
+        if (l >= off) {
+          B = __fmaf_rn(A, Bp, B);
+          A = __fmul_rn(A, Ap);
+        }
+      }
+      float C = __shfl_up_sync(FULL, B, 1);
+      if (l == 0) C = 0.0f;
+      float xl = 0.0f, ql = 1.0f;
+#pragma unroll
+      for (int k = MX - 1; k >= 0; k--) {
+        const int j = jb + k;
+        if (j < n) {
+          const float q = sq[j];
+          xl = __fmaf_rn(q, xl, __fmaf_rn(pm[k], C, d[k]));
+          ql = __fmul_rn(ql, q);
+          d[k] = xl;
+          pm[k] = ql;
+        }
+      }
+      // suffix scan of the maps X -> ql X + xl (the last row's q = 0)
+      A = ql;
+      B = xl;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const float Ap = __shfl_down_sync(FULL, A, off), Bp = __shfl_down_sync(FULL, B, off);
+        if (l + off < 32) {
+          B = __fmaf_rn(A, Bp, B);
+          A = __fmul_rn(A, Ap);
+        }
+      }
+      float X = __shfl_down_sync(FULL, B, 1);
+      if (l == 31) X = 0.0f;
+#pragma unroll
+      for (int k = 0; k < MX; k++) {
+        const int j = jb + k;
+        if (j < n) sr[j] = __fmaf_rn(pm[k], X, d[k]);
+      }
+    }
+
+    // ---- copy out (or add to the state)
+    if (D == 0) {
+      __syncwarp();
+      if (solve) {
+#pragma unroll
+        for (int k = 0; k < MX; k++) {
+          const int j = l + 32 * k;
+          if (j < n) f[L.base + j] = sr[j];
+        }
+      }
+    } else {
+      __syncthreads();
+      if (stc) {
+        const long long s32 = 32 * Lc.s;
+        const long long g0 = Lc.base + (long long)jc * Lc.s;
+        if (ACC) {
+          // all of this thread's state loads are issued before its stores
+          double uv[MX];
+#pragma unroll
+          for (int m = 0; m < MX; m++)
+            if (jc + 32 * m < n) uv[m] = u[g0 + m * s32];
+#pragma unroll
+          for (int m = 0; m < MX; m++)
+            if (jc + 32 * m < n) u[g0 + m * s32] = uv[m] + (double)cr[jc + 32 * m];
+        } else {
+#pragma unroll
+          for (int m = 0; m < MX; m++)
+            if (jc + 32 * m < n) f[g0 + m * s32] = cr[jc + 32 * m];
+        }
+      }
+    }
+  }
 }
 
 // u^{n+1} = u^n + d, four nodes per thread
@@ -491,18 +778,100 @@ __global__ void __launch_bounds__(256) k_accumulate(double* __restrict__ u, cons
   }
 }
 
+// Longest line of the segmented solves: 32 lanes of 17 rows.
+constexpr int kSegMaxRows = 32 * 17;
+
+// Shape of the FP32 ring sweeps (rows per chunk, ring chunks, threads per
+// CTA), for lines longer than that: 448 threads on each of the 148 SMs
+// cover the 66,049 lines of a 257^3 grid in one wave.
+constexpr int S32_CH = 8, S32_NS = 4, S32_NT = 448;
+
+template <int D, int MX>
+void launch_wline(const Dev& P, float* f, double* u, cudaStream_t st) {
+  constexpr size_t smem = wline_smem<MX>();
+  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
+  const long long need = (nlines<D>(P) + WL_WARPS - 1) / WL_WARPS;
+  const unsigned grid = (unsigned)std::min<long long>(need, (long long)P.sweep_blocks * per_sm);
+  if (D == 2 && u)
+    k_wline32<2, MX, true><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, u);
+  else
+    k_wline32<D, MX, false><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, nullptr);
+}
+
+template <int D>
+void launch_wline_n(const Dev& P, float* f, double* u, cudaStream_t st) {
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  if (nd <= 32 * 3)
+    launch_wline<D, 3>(P, f, u, st);
+  else if (nd <= 32 * 5)
+    launch_wline<D, 5>(P, f, u, st);
+  else if (nd <= 32 * 9)
+    launch_wline<D, 9>(P, f, u, st);
+  else if (nd <= 32 * 13)
+    launch_wline<D, 13>(P, f, u, st);
+  else
+    launch_wline<D, 17>(P, f, u, st);
+}
+
+template <int D>
+void sweep32(const Dev& P, float* f, double* u, cudaStream_t st) {
+  const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  const bool seg = P.cib[D] != nullptr;  // coefficients built: the lines fit the segmented solves
+  if (P.nblk[D] > 0) {
+    if (seg)
+      k_block_rhs32<D, true><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
+    else
+      k_block_rhs32<D, false><<<(P.nblk[D] + TPB - 1) / TPB, TPB, 0, st>>>(P, f, P.nblk[D]);
+  }
+  if (seg) {
+    launch_wline_n<D>(P, f, u, st);
+    return;
+  }
+  k_sweep32<D, S32_CH, S32_NS, S32_NT>
+      <<<sweep_grid(P, nlines<D>(P), S32_NT), S32_NT, shape32_smem<S32_CH, S32_NS, S32_NT>(nd), st>>>(P, f);
+  if (D == 2 && u) {
+    const long long nn = P.nn;
+    k_accumulate<<<4 * P.sweep_blocks * 4, 256, 0, st>>>(u, f, nn);
+  }
+}
+
 }  // namespace
+
+template <int D, int MX, bool ACC>
+void allow_smem() {
+  cudaFuncSetAttribute(k_wline32<D, MX, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wline_smem<MX>());
+}
 
 void configure_mixed_kernels() {
   constexpr int smem = 232448;
   cudaFuncSetAttribute(k_sweep32<0, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_sweep32<1, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_sweep32<2, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  allow_smem<0, 13, false>();
+  allow_smem<1, 13, false>();
+  allow_smem<2, 13, false>();
+  allow_smem<2, 13, true>();
+  allow_smem<0, 17, false>();
+  allow_smem<1, 17, false>();
+  allow_smem<2, 17, false>();
+  allow_smem<2, 17, true>();
 }
 
 int mixed_sweep_threads() { return S32_NT; }
 
 bool mixed_shape_fits(int nmax) { return shape32_smem<S32_CH, S32_NS, S32_NT>(nmax) <= (size_t)232448; }
+
+bool mixed_segments_fit(int n) { return n <= kSegMaxRows; }
+
+int build_mixed_coefs(const Dev& P, cudaStream_t st) {
+  k_coef32<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P);
+  k_coef32<1><<<(unsigned)((nlines<1>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P);
+  k_coef32<2><<<(unsigned)((nlines<2>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P);
+  k_ctab32<0><<<(2 * P.nx + TPB - 1) / TPB, TPB, 0, st>>>(P);
+  k_ctab32<1><<<(2 * P.ny + TPB - 1) / TPB, TPB, 0, st>>>(P);
+  k_ctab32<2><<<(2 * P.nz + TPB - 1) / TPB, TPB, 0, st>>>(P);
+  return 6;
+}
 
 int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t st, cudaEvent_t* ev) {
   int launches = 0;
@@ -526,16 +895,15 @@ int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t 
   }
   mark(1);
   mark(0);
-  sweep32<0>(P, P.r32, st);
+  sweep32<0>(P, P.r32, nullptr, st);
   mark(1);
   mark(0);
-  sweep32<1>(P, P.r32, st);
+  sweep32<1>(P, P.r32, nullptr, st);
   mark(1);
   mark(0);
-  sweep32<2>(P, P.r32, st);
-  k_accumulate<<<4 * P.sweep_blocks * 4, 256, 0, st>>>(u, P.r32, P.nn);
+  sweep32<2>(P, P.r32, u, st);
   mark(1);
-  launches += 4;
+  launches += P.cib[2] ? 3 : 4;
   for (int d = 0; d < 3; d++) launches += P.nblk[d] > 0;
   return launches;
 }

@@ -78,11 +78,10 @@ class Server:
         self.batches = 0
 
     # -- pool tasks ----------------------------------------------------------
-    @staticmethod
-    def _setup(job: _Job) -> _Job:
+    def _setup(self, job: _Job) -> _Job:
         tags, cr, _ = setup_host(job.req.spec)
         job.tags, job.crossings = tags, cr
-        job.bound = device_bytes_bound(job.req.spec, len(cr))
+        job.bound = device_bytes_bound(job.req.spec, len(cr), precision=self.precision)
         return job
 
     def _upload(self, job: _Job) -> _Job:

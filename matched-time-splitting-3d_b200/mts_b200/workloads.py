@@ -67,11 +67,13 @@ def served_requests(count: int, rate: float, seed: int = 0) -> list[Request]:
     return out
 
 
-def device_bytes_bound(spec: Spec, ncrossings: int, sms: int = 148) -> int:
+def device_bytes_bound(spec: Spec, ncrossings: int, sms: int = 148, precision: str = "plain") -> int:
     """An upper bound on the device memory mts_create allocates for `spec`
     with `ncrossings` crossings (the layout of the library's allocations: two
     FP64 fields, FP64 and FP32 per-node factors for every direction, the FP32
-    increment, both d' scratches, the tables and the MIB data)."""
+    increment, both d' scratches, the tables and the MIB data), plus, for the
+    mixed form, the segmented solves' per-node coefficients (three FP32
+    values per node and direction, built when the form is switched on)."""
     nx, ny, nz = spec.n
     N = nx * ny * nz
     nmax = max(spec.n)
@@ -90,4 +92,6 @@ def device_bytes_bound(spec: Spec, ncrossings: int, sms: int = 148) -> int:
     b += 3 * 2 * 2 * 12 * nmax + 3 * 3 * 8 * nmax  # prefix tables, axis tables
     b += ncrossings * (432 + 3 * 12 + 88 + 16 + 3 * 8)  # blocks, block RHS, constants, jumps, MIB nodes
     b += 4096 * 3 * 8 + 64                        # norm partials
+    if precision == "mixed" and spec.method == "adi" and nmax <= 544:
+        b += 3 * 3 * 4 * N                        # cib, cp, cq per direction
     return int(b * 1.02) + (1 << 20)

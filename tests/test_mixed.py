@@ -54,6 +54,29 @@ def test_mixed_beta_ratios_anisotropic(beta_out):
     assert l_m <= LINF_RATIO * l_p
 
 
+def test_mixed_long_lines_take_the_ring_sweeps():
+    """Lines too long for the segmented tiles' shared memory (600 rows in x)
+    take the ring sweeps, the others (17 rows) the tiles, in one step."""
+    spec = M.Spec(n=(600, 17, 17), surface="ellipsoid", surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
+                  beta_in=1.0, beta_out=10.0, method="adi", mib=2, dt=2.0 / 16)
+    u_p, (l_p, _, _) = run(spec, "plain", 4)
+    u_m, (l_m, _, _) = run(spec, "mixed", 4)
+    assert rel_maxdiff(u_m, u_p) <= REL_TOL
+    assert l_m <= LINF_RATIO * l_p
+
+
+@pytest.mark.parametrize("n", [(17, 17, 17), (33, 65, 129), (257, 257, 257)])
+def test_mixed_segment_edges(n):
+    """Line lengths that leave the last segments short or empty (17 rows over
+    8 segments of 3), mixed lengths per direction, and the bench grid."""
+    spec = M.Spec(n=n, surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, method="adi",
+                  mib=2, dt=2.0 / (max(n) - 1))
+    u_p, (l_p, _, _) = run(spec, "plain", 3)
+    u_m, (l_m, _, _) = run(spec, "mixed", 3)
+    assert rel_maxdiff(u_m, u_p) <= REL_TOL
+    assert l_m <= LINF_RATIO * l_p
+
+
 def test_mixed_rejects_other_methods():
     spec = M.Spec(n=(33, 33, 33), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=10.0,
                   method="lod-cn", mib=2, dt=1.0 / 16)

@@ -38,3 +38,18 @@ def test_device_bytes_bound_holds(n):
     with M.Solver(spec, tags=tags, crossings=cr) as s:
         used = s.device_bytes()
     assert used <= bound <= 1.5 * used + (4 << 20), (used, bound)
+
+
+@pytest.mark.parametrize("n", [(33, 49, 65), (129, 129, 129)])
+def test_device_bytes_bound_holds_mixed(n):
+    """The bound with the mixed form's per-node coefficients, which the
+    library allocates when the form is switched on."""
+    from dataclasses import replace
+
+    spec = replace(draw_problem(np.random.default_rng(6), n=n), method="adi")
+    tags, cr, _ = M.setup_host(spec)
+    bound = device_bytes_bound(spec, len(cr), precision="mixed")
+    with M.Solver(spec, tags=tags, crossings=cr) as s:
+        s.set_precision("mixed")
+        used = s.device_bytes()
+    assert used <= bound <= 1.5 * used + (4 << 20), (used, bound)

@@ -53,7 +53,7 @@ def fakes(monkeypatch):
     monkeypatch.setattr(serve, "Solver", FakeSolver)
     monkeypatch.setattr(serve, "batch_advance_steps", fake_batch)
     monkeypatch.setattr(serve, "setup_host", lambda spec: (None, np.zeros(4), None))
-    monkeypatch.setattr(serve, "device_bytes_bound", lambda spec, nc: 100)
+    monkeypatch.setattr(serve, "device_bytes_bound", lambda spec, nc, **kw: 100)
     FakeSolver.live = FakeSolver.peak = 0
 
 
