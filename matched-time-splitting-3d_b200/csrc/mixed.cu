@@ -551,209 +551,247 @@ __global__ void __launch_bounds__(TPB) k_ctab32(const __grid_constant__ Dev P) {
   T[2 * n + j] = (float)(-gn);
 }
 
-// One warp per line, every direction.  A line's rows (right-hand side, and
-// for a crossing line its 1/bet, p, q) are copied into the warp's
-// shared-memory rows; lane l runs rows [l MX, l MX + MX) (MX odd: the lanes'
-// stride falls on distinct banks); the segment carries are warp scans
-// (shuffles) of the affine end maps; the solution goes back out through the
-// same rows.  x lines are contiguous, so a warp copies its own line.  y and
-// z lines are strided, so the CTA copies its 8 lines together, 8 neighbours
-// (32 bytes) per row at a time.
-// ACC (z): the increment is added to the FP64 state instead of being stored,
-// face lines included, so that u^{n+1} = u^n + d at every node.
 constexpr int WL_WARPS = 8;
 
 template <int MX>
-constexpr size_t wline_smem() {
-  // row tables 2 x 3 x R, then per warp r, ib, p, q (R each) + 4 floats of bank padding
+constexpr size_t xline_smem() {
+  // row tables 2 x 3 x R, then per warp r, ib, p, q (R each) + 4 floats
   return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)WL_WARPS * (4 * 32 * MX + 4));
 }
 
-template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * WL_WARPS) k_wline32(const __grid_constant__ Dev P, float* __restrict__ f,
-                                                         double* __restrict__ u) {
-  static_assert(MX & 1, "odd rows per lane");
-  static_assert(!ACC || D == 2, "the increment is accumulated after the z solve");
-  constexpr int R = 32 * MX;
-  constexpr int LS = 4 * R + 4;  // a warp's rows: 4 fields of R, and padding so that the
-                                 // 8 lines of a cooperative copy fall on distinct banks
+// A warp solves one line held in shared memory: rows sr[j] (right-hand side
+// in, solution out) with 1/bet, p, q in si, sp, sq (by row).  Lane l runs
+// rows [l MX, l MX + MX) (MX odd: the lanes' stride falls on distinct
+// banks); the segment carries are warp scans (shuffles) of the affine end
+// maps.
+template <int MX>
+__device__ __forceinline__ void solve_line32(float* sr, const float* si, const float* sp, const float* sq, int n,
+                                             int l) {
   constexpr unsigned FULL = 0xffffffffu;
+  const int jb = l * MX;
+  float d[MX], pm[MX];
+  float dl = 0.0f, pl = 1.0f;
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    const int j = jb + k;
+    if (j < n) {
+      const float p = sp[j];
+      dl = __fmaf_rn(p, dl, __fmul_rn(sr[j], si[j]));
+      pl = __fmul_rn(pl, p);
+      d[k] = dl;
+      pm[k] = pl;
+    }
+  }
+  // inclusive scan of the maps c -> pl c + dl over the lanes; the carry into
+  // lane l is the composition over lanes < l applied to 0 (lane 0 starts at
+  // face row 0, whose p = 0)
+  float A = pl, B = dl;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const float Ap = __shfl_up_sync(FULL, A, off), Bp = __shfl_up_sync(FULL, B, off);
+    if (l >= off) {
+      B = __fmaf_rn(A, Bp, B);
+      A = __fmul_rn(A, Ap);
+    }
+  }
+  float C = __shfl_up_sync(FULL, B, 1);
+  if (l == 0) C = 0.0f;
+  float xl = 0.0f, ql = 1.0f;
+#pragma unroll
+  for (int k = MX - 1; k >= 0; k--) {
+    const int j = jb + k;
+    if (j < n) {
+      const float q = sq[j];
+      xl = __fmaf_rn(q, xl, __fmaf_rn(pm[k], C, d[k]));
+      ql = __fmul_rn(ql, q);
+      d[k] = xl;
+      pm[k] = ql;
+    }
+  }
+  // suffix scan of the maps X -> ql X + xl (the last row's q = 0)
+  A = ql;
+  B = xl;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const float Ap = __shfl_down_sync(FULL, A, off), Bp = __shfl_down_sync(FULL, B, off);
+    if (l + off < 32) {
+      B = __fmaf_rn(A, Bp, B);
+      A = __fmul_rn(A, Ap);
+    }
+  }
+  float X = __shfl_down_sync(FULL, B, 1);
+  if (l == 31) X = 0.0f;
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    const int j = jb + k;
+    if (j < n) sr[j] = __fmaf_rn(pm[k], X, d[k]);
+  }
+}
+
+// Row tables into shared memory: [side][ib, p, q][R].
+__device__ __forceinline__ void load_row_tables(float* tab, const float* ctab, int n, int R) {
+  for (int i = threadIdx.x; i < 6 * n; i += blockDim.x) tab[(i / n) * R + i % n] = ctab[i];
+}
+
+// x lines: contiguous in memory, so a warp copies its own line in and out.
+template <int MX>
+__global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant__ Dev P, float* __restrict__ f) {
+  static_assert(MX & 1, "odd rows per lane");
+  constexpr int R = 32 * MX;
+  constexpr int LS = 4 * R + 4;
   extern __shared__ float sw[];
-  const int n = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  const int n = P.nx;
   float* const tab = sw;  // [side][ib, p, q][R]
-  float* const buf = sw + 6 * R;
-  for (int i = threadIdx.x; i < 6 * n; i += 32 * WL_WARPS) tab[(i / n) * R + i % n] = P.ctab[D][i];
+  load_row_tables(tab, P.ctab[0], n, R);
   __syncthreads();
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  float* const sr = buf + w * LS;
+  float* const sr = sw + 6 * R + w * LS;
+  const long long nl = nlines<0>(P);
+  const float* __restrict__ cib = P.cib[0];
+  const float* __restrict__ cpp = P.cp[0];
+  const float* __restrict__ cqq = P.cq[0];
+  for (long long t = (long long)blockIdx.x * WL_WARPS + w; t < nl; t += (long long)gridDim.x * WL_WARPS) {
+    Line L;
+    decode_line<0>(P, t, L);
+    if (L.boundary) continue;  // face line: its right-hand side is its solution (warp-uniform)
+    const bool cross = P.bstart[0][L.lid + 1] > P.bstart[0][L.lid];
+    const int side0 = (P.lside[0][L.lid] >> 1) & 1;
+    __syncwarp();  // the previous line's stores have read the rows
+#pragma unroll
+    for (int k = 0; k < MX; k++) {
+      const int j = l + 32 * k;
+      if (j < n) {
+        const long long g = L.base + j;
+        cp_async4(sr + j, f + g);
+        if (cross) {
+          cp_async4(sr + R + j, cib + g);
+          cp_async4(sr + 2 * R + j, cpp + g);
+          cp_async4(sr + 3 * R + j, cqq + g);
+        }
+      }
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp();
+    const float* const si = cross ? sr + R : tab + side0 * 3 * R;
+    solve_line32<MX>(sr, si, si + R, si + 2 * R, n, l);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < MX; k++) {
+      const int j = l + 32 * k;
+      if (j < n) f[L.base + j] = sr[j];
+    }
+  }
+}
+
+// y and z lines: strided, so the CTA copies 8 neighbouring lines together, 8
+// neighbours (32 bytes) of a row at a time, and warp w solves line w.  (A
+// second buffer, to copy the next 8 lines in while these are solved, was
+// measured slower: it halves the CTAs an SM holds, and they already overlap
+// one another's copies.)
+// ACC (z): the FP64 state is copied in with the right-hand side and the
+// increment is added to it instead of being stored, face lines included, so
+// that u^{n+1} = u^n + d at every node.
+template <int MX, bool ACC>
+constexpr size_t yzline_smem() {
+  // row tables 2 x 3 x R; 8 lines x (r, ib, p, q: R each + 4 floats of bank
+  // padding); ACC: 8 lines x (R + 4) doubles
+  return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)WL_WARPS * (4 * 32 * MX + 4)) +
+         (ACC ? sizeof(double) * WL_WARPS * (32 * MX + 4) : 0);
+}
+
+template <int D, int MX, bool ACC>
+__global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
+                                                          double* __restrict__ u) {
+  static_assert(MX & 1, "odd rows per lane");
+  static_assert(D != 0 && (!ACC || D == 2), "y and z lines; accumulation after the z solve");
+  constexpr int R = 32 * MX;
+  constexpr int LS = 4 * R + 4;  // padding: the 8 lines of a copy instruction fall on distinct banks
+  extern __shared__ float sw[];
+  const int n = D == 1 ? P.ny : P.nz;
+  float* const tab = sw;
+  load_row_tables(tab, P.ctab[D], n, R);
+  float* const buf0 = sw + 6 * R;  // [8][LS]
+  // (the float offset 6 R + 8 LS = 38 R + 32 is even: 8-byte aligned)
+  double* const ubuf0 = reinterpret_cast<double*>(buf0 + WL_WARPS * LS);  // [8][R + 4]
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int c = threadIdx.x & 7, jc = threadIdx.x >> 3;  // this thread's share of a copy: line c, rows jc + 32 m
   const long long nl = nlines<D>(P);
+  const long long stride = (long long)gridDim.x * WL_WARPS;
   const float* __restrict__ cib = P.cib[D];
   const float* __restrict__ cpp = P.cp[D];
   const float* __restrict__ cqq = P.cq[D];
-  const int jb = l * MX;
-  // y, z: this thread's share of the cooperative copies, line c of the 8
-  const int c = threadIdx.x & 7, jc = threadIdx.x >> 3;
-  float* const cr = buf + c * LS;
 
-  for (long long t0 = (long long)blockIdx.x * WL_WARPS; t0 < nl; t0 += (long long)gridDim.x * WL_WARPS) {
+  // line c of the tile at t0: where it is and what to copy
+  struct Copy {
+    long long g0, s32;  // row jc of the line, 32 rows
+    bool st, cross;
+  };
+  auto copy_in = [&](long long t0) -> Copy {
+    Copy cp{0, 0, false, false};
+    const long long tc = t0 + c;
+    if (tc < nl) {
+      Line Lc;
+      decode_line<D>(P, tc, Lc);
+      cp.st = !Lc.boundary || ACC;  // (ACC) face lines pass their right-hand side through
+      cp.cross = !Lc.boundary && P.bstart[D][Lc.lid + 1] > P.bstart[D][Lc.lid];
+      cp.g0 = Lc.base + (long long)jc * Lc.s;
+      cp.s32 = 32 * Lc.s;
+    }
+    float* const cr = buf0 + c * LS;
+    double* const cu = ubuf0 + c * (R + 4);
+    if (cp.st) {
+#pragma unroll
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) {
+          const long long g = cp.g0 + m * cp.s32;
+          cp_async4(cr + j, f + g);
+          if (ACC) cp_async8(cu + j, u + g);
+          if (cp.cross) {
+            cp_async4(cr + R + j, cib + g);
+            cp_async4(cr + 2 * R + j, cpp + g);
+            cp_async4(cr + 3 * R + j, cqq + g);
+          }
+        }
+      }
+    }
+    cp_async_commit();
+    return cp;
+  };
+
+  for (long long t0 = (long long)blockIdx.x * WL_WARPS; t0 < nl; t0 += stride) {
+    // a thread copies into exactly the rows it stored from last time: no
+    // barrier needed before the copy
+    const Copy cur = copy_in(t0);
+    cp_async_wait<0>();
+    __syncthreads();  // every thread's copies are in
+    // warp w: line t0 + w
     const long long t = t0 + w;
-    const bool act = t < nl;
-    Line L;
-    decode_line<D>(P, act ? t : nl - 1, L);
-    const bool solve = act && !L.boundary;  // uniform over the warp
-    bool cross = false;
-    int side0 = 0;
-    if (solve) {
-      cross = P.bstart[D][L.lid + 1] > P.bstart[D][L.lid];
-      side0 = (P.lside[D][L.lid] >> 1) & 1;
-    }
-
-    // ---- copy in
-    Line Lc;
-    bool stc = false;
-    if (D == 0) {
-      __syncwarp();  // the previous line's stores have read the rows
-      if (solve) {
-#pragma unroll
-        for (int k = 0; k < MX; k++) {
-          const int j = l + 32 * k;
-          if (j < n) {
-            const long long g = L.base + j;
-            cp_async4(sr + j, f + g);
-            if (cross) {
-              cp_async4(sr + R + j, cib + g);
-              cp_async4(sr + 2 * R + j, cpp + g);
-              cp_async4(sr + 3 * R + j, cqq + g);
-            }
-          }
-        }
+    if (t < nl) {
+      Line L;
+      decode_line<D>(P, t, L);
+      if (!L.boundary) {
+        const bool cross = P.bstart[D][L.lid + 1] > P.bstart[D][L.lid];
+        const int side0 = (P.lside[D][L.lid] >> 1) & 1;
+        float* const sr = buf0 + w * LS;
+        const float* const si = cross ? sr + R : tab + side0 * 3 * R;
+        solve_line32<MX>(sr, si, si + R, si + 2 * R, n, l);
       }
-      cp_async_commit();
-      cp_async_wait<0>();
-      __syncwarp();
-    } else {
-      const long long tc = t0 + c;
-      const bool actc = tc < nl;
-      decode_line<D>(P, actc ? tc : nl - 1, Lc);
-      const bool solvec = actc && !Lc.boundary;
-      stc = solvec || (ACC && actc);  // (ACC) face lines pass their right-hand side through
-      const bool crossc = solvec && P.bstart[D][Lc.lid + 1] > P.bstart[D][Lc.lid];
-      __syncthreads();  // the previous lines' stores have read the rows
-      if (stc) {
-        const long long s32 = 32 * Lc.s;
-        const float* gf = f + Lc.base + (long long)jc * Lc.s;
-#pragma unroll
-        for (int m = 0; m < MX; m++) {
-          const int j = jc + 32 * m;
-          if (j < n) {
-            const long long o = m * s32;
-            cp_async4(cr + j, gf + o);
-            if (crossc) {
-              const long long g = (gf - f) + o;
-              cp_async4(cr + R + j, cib + g);
-              cp_async4(cr + 2 * R + j, cpp + g);
-              cp_async4(cr + 3 * R + j, cqq + g);
-            }
-          }
-        }
-      }
-      cp_async_commit();
-      cp_async_wait<0>();
-      __syncthreads();
     }
-
-    // ---- solve this warp's line
-    if (solve) {
-      const float* const si = cross ? sr + R : tab + side0 * 3 * R;
-      const float* const sp = si + R;
-      const float* const sq = sp + R;
-      float d[MX], pm[MX];
-      float dl = 0.0f, pl = 1.0f;
+    __syncthreads();
+    if (cur.st) {
+      const float* const cr = buf0 + c * LS;
+      const double* const cu = ubuf0 + c * (R + 4);
 #pragma unroll
-      for (int k = 0; k < MX; k++) {
-        const int j = jb + k;
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
         if (j < n) {
-          const float p = sp[j];
-          dl = __fmaf_rn(p, dl, __fmul_rn(sr[j], si[j]));
-          pl = __fmul_rn(pl, p);
-          d[k] = dl;
-          pm[k] = pl;
-        }
-      }
-      // inclusive scan of the maps c -> pl c + dl over the lanes; the carry
-      // into lane l is the composition over lanes < l applied to 0 (lane 0
-      // starts at face row 0, whose p = 0)
-      float A = pl, B = dl;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const float Ap = __shfl_up_sync(FULL, A, off), Bp = __shfl_up_sync(FULL, B, off);
-        if (l >= off) {
-          B = __fmaf_rn(A, Bp, B);
-          A = __fmul_rn(A, Ap);
-        }
-      }
-      float C = __shfl_up_sync(FULL, B, 1);
-      if (l == 0) C = 0.0f;
-      float xl = 0.0f, ql = 1.0f;
-#pragma unroll
-      for (int k = MX - 1; k >= 0; k--) {
-        const int j = jb + k;
-        if (j < n) {
-          const float q = sq[j];
-          xl = __fmaf_rn(q, xl, __fmaf_rn(pm[k], C, d[k]));
-          ql = __fmul_rn(ql, q);
-          d[k] = xl;
-          pm[k] = ql;
-        }
-      }
-      // suffix scan of the maps X -> ql X + xl (the last row's q = 0)
-      A = ql;
-      B = xl;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const float Ap = __shfl_down_sync(FULL, A, off), Bp = __shfl_down_sync(FULL, B, off);
-        if (l + off < 32) {
-          B = __fmaf_rn(A, Bp, B);
-          A = __fmul_rn(A, Ap);
-        }
-      }
-      float X = __shfl_down_sync(FULL, B, 1);
-      if (l == 31) X = 0.0f;
-#pragma unroll
-      for (int k = 0; k < MX; k++) {
-        const int j = jb + k;
-        if (j < n) sr[j] = __fmaf_rn(pm[k], X, d[k]);
-      }
-    }
-
-    // ---- copy out (or add to the state)
-    if (D == 0) {
-      __syncwarp();
-      if (solve) {
-#pragma unroll
-        for (int k = 0; k < MX; k++) {
-          const int j = l + 32 * k;
-          if (j < n) f[L.base + j] = sr[j];
-        }
-      }
-    } else {
-      __syncthreads();
-      if (stc) {
-        const long long s32 = 32 * Lc.s;
-        const long long g0 = Lc.base + (long long)jc * Lc.s;
-        if (ACC) {
-          // all of this thread's state loads are issued before its stores
-          double uv[MX];
-#pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) uv[m] = u[g0 + m * s32];
-#pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) u[g0 + m * s32] = uv[m] + (double)cr[jc + 32 * m];
-        } else {
-#pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) f[g0 + m * s32] = cr[jc + 32 * m];
+          const long long g = cur.g0 + m * cur.s32;
+          if (ACC)
+            u[g] = cu[j] + (double)cr[j];
+          else
+            f[g] = cr[j];
         }
       }
     }
@@ -788,14 +826,22 @@ constexpr int S32_CH = 8, S32_NS = 4, S32_NT = 448;
 
 template <int D, int MX>
 void launch_wline(const Dev& P, float* f, double* u, cudaStream_t st) {
-  constexpr size_t smem = wline_smem<MX>();
-  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
   const long long need = (nlines<D>(P) + WL_WARPS - 1) / WL_WARPS;
+  if (D == 0) {
+    constexpr size_t smem = xline_smem<MX>();
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
+    const unsigned grid = (unsigned)std::min<long long>(need, (long long)P.sweep_blocks * per_sm);
+    k_xline32<MX><<<grid, 32 * WL_WARPS, smem, st>>>(P, f);
+    return;
+  }
+  const bool acc = D == 2 && u;
+  const size_t smem = acc ? yzline_smem<MX, true>() : yzline_smem<MX, false>();
+  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
   const unsigned grid = (unsigned)std::min<long long>(need, (long long)P.sweep_blocks * per_sm);
-  if (D == 2 && u)
-    k_wline32<2, MX, true><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, u);
+  if (acc)
+    k_yzline32<2, MX, true><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, u);
   else
-    k_wline32<D, MX, false><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, nullptr);
+    k_yzline32<D == 0 ? 1 : D, MX, false><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, nullptr);
 }
 
 template <int D>
@@ -837,9 +883,15 @@ void sweep32(const Dev& P, float* f, double* u, cudaStream_t st) {
 
 }  // namespace
 
-template <int D, int MX, bool ACC>
+template <int MX>
 void allow_smem() {
-  cudaFuncSetAttribute(k_wline32<D, MX, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wline_smem<MX>());
+  cudaFuncSetAttribute(k_xline32<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xline_smem<MX>());
+  cudaFuncSetAttribute(k_yzline32<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<MX, false>());
+  cudaFuncSetAttribute(k_yzline32<2, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<MX, false>());
+  cudaFuncSetAttribute(k_yzline32<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<MX, true>());
 }
 
 void configure_mixed_kernels() {
@@ -847,14 +899,11 @@ void configure_mixed_kernels() {
   cudaFuncSetAttribute(k_sweep32<0, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_sweep32<1, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(k_sweep32<2, S32_CH, S32_NS, S32_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  allow_smem<0, 13, false>();
-  allow_smem<1, 13, false>();
-  allow_smem<2, 13, false>();
-  allow_smem<2, 13, true>();
-  allow_smem<0, 17, false>();
-  allow_smem<1, 17, false>();
-  allow_smem<2, 17, false>();
-  allow_smem<2, 17, true>();
+  allow_smem<3>();
+  allow_smem<5>();
+  allow_smem<9>();
+  allow_smem<13>();
+  allow_smem<17>();
 }
 
 int mixed_sweep_threads() { return S32_NT; }
