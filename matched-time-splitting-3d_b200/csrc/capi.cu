@@ -69,6 +69,7 @@ struct mts_problem {
   int64_t device_bytes = 0;  // sum of the allocations' sizes
   double* norm_part = nullptr;
   double* norm_out = nullptr;
+  mts::SideStream side{nullptr, nullptr, nullptr};  // the mixed form's second stream
 
   int norm_nb = 1;
   double t = 0;
@@ -92,6 +93,10 @@ struct mts_problem {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
     }
+    // every step joins the side stream back into the main one before it ends
+    if (side.stream) cudaStreamDestroy(side.stream);
+    if (side.fork) cudaEventDestroy(side.fork);
+    if (side.join) cudaEventDestroy(side.join);
   }
   template <class T>
   cudaError_t put(T** dst, const T* src, size_t n) {
@@ -638,7 +643,7 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
     ev = h->ev_busy.back().data();
   }
   if (h->dev.precision == 1)
-    h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev);
+    h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev, &h->side);
   else
     h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev);
   cudaError_t e = cudaGetLastError();
@@ -933,7 +938,7 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     if (h->dev.precision != 1) continue;
     for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
-      h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr);
+      h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
       mts::launch_tick(h->dev, h->stream);
       h->launches++;
     }
@@ -1162,6 +1167,11 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
       }
       mts::build_mixed_coefs(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
+    }
+    if (!h->side.stream) {
+      CUDA_TRY(cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming));
+      CUDA_TRY(cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming));
     }
   }
   h->dev.precision = precision;

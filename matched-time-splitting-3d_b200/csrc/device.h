@@ -153,7 +153,14 @@ int launch_initialize(const Dev& P, double E, double* u, cudaStream_t stream);
 int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t stream,
                 cudaEvent_t* ev);
 // The mixed-precision Douglas-ADI step (mixed.cu), in place on u.
-int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t stream, cudaEvent_t* ev);
+// A second stream with its fork and join events (timing off), for work of a
+// step that can run beside the main stream's.
+struct SideStream {
+  cudaStream_t stream;
+  cudaEvent_t fork, join;
+};
+int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t stream, cudaEvent_t* ev,
+                      const SideStream* side);
 void configure_mixed_kernels();
 int mixed_sweep_threads();            // threads per CTA of the FP32 sweeps
 bool mixed_shape_fits(int nmax);      // their shared memory within the limit

@@ -695,9 +695,10 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant
 template <int MX, bool ACC>
 constexpr size_t yzline_smem() {
   // row tables 2 x 3 x R; 8 lines x (r, ib, p, q: R each + 4 floats of bank
-  // padding); ACC: 8 lines x (R + 4) doubles
+  // padding); ACC: 8 lines x (R + 2) doubles (the 2: a half warp's 8-byte
+  // accesses, 8 lines x 2 rows, fall on distinct bank pairs)
   return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)WL_WARPS * (4 * 32 * MX + 4)) +
-         (ACC ? sizeof(double) * WL_WARPS * (32 * MX + 4) : 0);
+         (ACC ? sizeof(double) * WL_WARPS * (32 * MX + 2) : 0);
 }
 
 template <int D, int MX, bool ACC>
@@ -713,7 +714,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
   load_row_tables(tab, P.ctab[D], n, R);
   float* const buf0 = sw + 6 * R;  // [8][LS]
   // (the float offset 6 R + 8 LS = 38 R + 32 is even: 8-byte aligned)
-  double* const ubuf0 = reinterpret_cast<double*>(buf0 + WL_WARPS * LS);  // [8][R + 4]
+  double* const ubuf0 = reinterpret_cast<double*>(buf0 + WL_WARPS * LS);  // [8][R + 2]
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int c = threadIdx.x & 7, jc = threadIdx.x >> 3;  // this thread's share of a copy: line c, rows jc + 32 m
   const long long nl = nlines<D>(P);
@@ -739,7 +740,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
       cp.s32 = 32 * Lc.s;
     }
     float* const cr = buf0 + c * LS;
-    double* const cu = ubuf0 + c * (R + 4);
+    double* const cu = ubuf0 + c * (R + 2);
     if (cp.st) {
 #pragma unroll
       for (int m = 0; m < MX; m++) {
@@ -782,7 +783,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
     __syncthreads();
     if (cur.st) {
       const float* const cr = buf0 + c * LS;
-      const double* const cu = ubuf0 + c * (R + 4);
+      const double* const cu = ubuf0 + c * (R + 2);
 #pragma unroll
       for (int m = 0; m < MX; m++) {
         const int j = jc + 32 * m;
@@ -922,27 +923,41 @@ int build_mixed_coefs(const Dev& P, cudaStream_t st) {
   return 6;
 }
 
-int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t st, cudaEvent_t* ev) {
+int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t st, cudaEvent_t* ev,
+                      const SideStream* side) {
   int launches = 0;
-  int slot = 0;
+  // The jumps and the residual's MIB rows (which read the jumps) run on the
+  // side stream, beside the pointwise residual: the two passes write
+  // disjoint nodes and read only the state.
+  const bool fork = side && side->stream && (P.ncross > 0 || P.nmibnode > 0);
+  cudaStream_t sst = fork ? side->stream : st;
+  if (fork) {
+    cudaEventRecord(side->fork, st);
+    cudaStreamWaitEvent(sst, side->fork, 0);
+  }
+  if (ev) cudaEventRecord(ev[0], sst);
+  if (P.ncross > 0) {
+    launch_jumps(P, T.e_next, sst);
+    launches++;
+  }
+  if (ev) cudaEventRecord(ev[1], sst);
+  if (ev) cudaEventRecord(ev[2], st);
+  if (P.nmibnode > 0) {
+    k_adi_resid_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, sst>>>(P, u, P.r32, T.e_next);
+    launches++;
+  }
+  k_adi_resid<2><<<pointwise_rows_grid(P), TPB, 0, st>>>(P, u, P.r32, T.e_next);
+  launches++;
+  if (fork) {
+    cudaEventRecord(side->join, sst);
+    cudaStreamWaitEvent(st, side->join, 0);
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  int slot = 2;
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[2 * slot + k], st);
     if (k == 1) slot++;
   };
-  mark(0);
-  if (P.ncross > 0) {
-    launch_jumps(P, T.e_next, st);
-    launches++;
-  }
-  mark(1);
-  mark(0);
-  k_adi_resid<2><<<pointwise_rows_grid(P), TPB, 0, st>>>(P, u, P.r32, T.e_next);
-  launches++;
-  if (P.nmibnode > 0) {
-    k_adi_resid_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u, P.r32, T.e_next);
-    launches++;
-  }
-  mark(1);
   mark(0);
   sweep32<0>(P, P.r32, nullptr, st);
   mark(1);
