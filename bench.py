@@ -60,7 +60,9 @@ ALG_BYTES = {
     "ts": {1: 17, 2: 17, 3: 17, 4: 17, 5: 17},
 }
 SLOT_NAMES = {
-    "adi": ["jumps", "adi_rhs", "adi_x_sweep", "adi_y_sweep", "adi_z_sweep"],
+    # ADI: the jumps (with the MIB rows of the first right-hand side) run on
+    # a side stream beside the pointwise pass; that slot's time overlaps the next
+    "adi": ["jumps_side_stream", "adi_rhs", "adi_x_sweep", "adi_y_sweep", "adi_z_sweep"],
     "lod-ie": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
     "lod-cn": ["jumps", "lod_x_sweep", "lod_y_sweep", "lod_z_sweep"],
     "ts": ["jumps", "ts_explicit_x", "ts_explicit_y", "ts_z_sweep", "ts_y_sweep", "ts_x_sweep"],

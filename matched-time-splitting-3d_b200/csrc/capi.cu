@@ -495,6 +495,13 @@ mts_status finish_create(mts_problem* h) {
     for (int k = 0; k < 3; k++) D.shape[k] = def;
   }
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (p.method == MTS_ADI) {
+    // Douglas-ADI steps run their jumps and MIB right-hand-side rows beside
+    // the pointwise pass, on this second stream
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming));
+  }
   // row slack of the fields the sweeps stage whole chunks of: kRowPad rows of
   // the largest stride (an x-y plane)
   const size_t fpad = (size_t)mts::kRowPad * (size_t)g.nx * (size_t)g.ny;
@@ -645,7 +652,7 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
   if (h->dev.precision == 1)
     h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev, &h->side);
   else
-    h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev);
+    h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev, &h->side);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MTS_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
   h->t = t_next;
@@ -1168,11 +1175,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
       mts::build_mixed_coefs(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
     }
-    if (!h->side.stream) {
-      CUDA_TRY(cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking));
-      CUDA_TRY(cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming));
-      CUDA_TRY(cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming));
-    }
+
   }
   h->dev.precision = precision;
   return MTS_OK;

@@ -150,15 +150,15 @@ struct StepTimes {
 // number of kernel launches made.
 int launch_initialize(const Dev& P, double E, double* u, cudaStream_t stream);
 // ev: null, or 2 events per kernel slot recorded around each launch.
-int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t stream,
-                cudaEvent_t* ev);
-// The mixed-precision Douglas-ADI step (mixed.cu), in place on u.
 // A second stream with its fork and join events (timing off), for work of a
 // step that can run beside the main stream's.
 struct SideStream {
   cudaStream_t stream;
   cudaEvent_t fork, join;
 };
+int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t stream,
+                cudaEvent_t* ev, const SideStream* side = nullptr);
+// The mixed-precision Douglas-ADI step (mixed.cu), in place on u.
 int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t stream, cudaEvent_t* ev,
                       const SideStream* side);
 void configure_mixed_kernels();

@@ -1044,19 +1044,30 @@ int launch_norms(const Dev& P, double E, const double* u, double* partial, int n
 
 // One time step.  u0 holds u^n on entry and u^{n+1} on return (the two
 // pointers are swapped when the result lands in the other buffer).
-int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t st, cudaEvent_t* ev) {
+int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cudaStream_t st, cudaEvent_t* ev,
+                const SideStream* side) {
   int launches = 0;
   int slot = 0;
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[2 * slot + k], st);
     if (k == 1) slot++;
   };
-  mark(0);
+  // Douglas-ADI: the jumps and the MIB rows of the first right-hand side
+  // (which read the jumps) run on the side stream beside its pointwise pass;
+  // the two passes write disjoint nodes and read only u^n.
+  const bool fork = side && side->stream && P.method == 0 && (P.ncross > 0 || P.nmibnode > 0);
+  cudaStream_t sst = fork ? side->stream : st;
+  if (fork) {
+    cudaEventRecord(side->fork, st);
+    cudaStreamWaitEvent(sst, side->fork, 0);
+  }
+  if (ev) cudaEventRecord(ev[0], sst);
   if (P.ncross > 0) {
-    k_jumps<<<(P.ncross + TPB - 1) / TPB, TPB, 0, st>>>(P, T.e_next);
+    k_jumps<<<(P.ncross + TPB - 1) / TPB, TPB, 0, sst>>>(P, T.e_next);
     launches++;
   }
-  mark(1);
+  if (ev) cudaEventRecord(ev[1], sst);
+  slot = 1;
   SweepIO io{};
   io.e1 = T.e_next;
   io.e0 = T.e_prev;
@@ -1067,10 +1078,14 @@ int launch_step(const Dev& P, const StepTimes& T, double*& u0, double*& u1, cuda
     // reads only its own nodes of u^n; its faces get Outer_u(t_next), the
     // value u** holds there).  The state stays in u0, u1 is scratch.
     mark(0);
-    k_adi_rhs<2><<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_next);
     if (P.nmibnode > 0) {
-      k_adi_rhs_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, st>>>(P, u0, u1, T.e_next);
+      k_adi_rhs_mib<<<(P.nmibnode + TPB - 1) / TPB, TPB, 0, sst>>>(P, u0, u1, T.e_next);
       launches++;
+    }
+    k_adi_rhs<2><<<pointwise_blocks(P), TPB, 0, st>>>(P, u0, u1, T.e_next);
+    if (fork) {
+      cudaEventRecord(side->join, sst);
+      cudaStreamWaitEvent(st, side->join, 0);
     }
     mark(1);
     io.stin = u1;
