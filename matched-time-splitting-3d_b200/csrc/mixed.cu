@@ -684,41 +684,57 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant
   }
 }
 
-// y and z lines: strided, so the CTA copies 8 neighbouring lines together, 8
-// neighbours (32 bytes) of a row at a time, and warp w solves line w.  (A
+// y and z lines: strided, so the CTA copies NL neighbouring lines together,
+// NL neighbours (4 NL bytes) of a row at a time, and warp w solves line w:
+// NL = 16 for y, 8 for z with the accumulation (whose FP64 state rows would
+// leave room for only one CTA of 16 per SM).  (A
 // second buffer, to copy the next 8 lines in while these are solved, was
 // measured slower: it halves the CTAs an SM holds, and they already overlap
 // one another's copies.)
 // ACC (z): the FP64 state is copied in with the right-hand side and the
 // increment is added to it instead of being stored, face lines included, so
 // that u^{n+1} = u^n + d at every node.
+template <bool ACC>
+__host__ __device__ constexpr int yz_lines() { return ACC ? 8 : 16; }
+// Padding of a line's rows so that a copy instruction's lanes (NL lines x
+// 32/NL rows) fall on distinct banks: 32/NL floats per line of (r, ib, p, q)
+// (line c starts at bank 32 c / NL), and 16/NL doubles per line of the FP64
+// state (a half warp's 8-byte accesses: NL lines x 16/NL rows).
+template <int NL>
+__host__ __device__ constexpr int yz_pad() { return 32 / NL; }
+template <int NL>
+__host__ __device__ constexpr int yz_upad() { return 16 / NL; }
+
 template <int MX, bool ACC>
 constexpr size_t yzline_smem() {
-  // row tables 2 x 3 x R; 8 lines x (r, ib, p, q: R each + 4 floats of bank
-  // padding); ACC: 8 lines x (R + 2) doubles (the 2: a half warp's 8-byte
-  // accesses, 8 lines x 2 rows, fall on distinct bank pairs)
-  return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)WL_WARPS * (4 * 32 * MX + 4)) +
-         (ACC ? sizeof(double) * WL_WARPS * (32 * MX + 2) : 0);
+  // row tables 2 x 3 x R; NL lines x (r, ib, p, q: R each + padding); ACC:
+  // NL lines x (R + padding) doubles
+  constexpr int NL = yz_lines<ACC>();
+  return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)NL * (4 * 32 * MX + yz_pad<NL>())) +
+         (ACC ? sizeof(double) * NL * (32 * MX + yz_upad<NL>()) : 0);
 }
 
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
+__global__ void __launch_bounds__(32 * yz_lines<ACC>()) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
                                                           double* __restrict__ u) {
   static_assert(MX & 1, "odd rows per lane");
   static_assert(D != 0 && (!ACC || D == 2), "y and z lines; accumulation after the z solve");
   constexpr int R = 32 * MX;
-  constexpr int LS = 4 * R + 4;  // padding: the 8 lines of a copy instruction fall on distinct banks
+  constexpr int NL = yz_lines<ACC>();
+  constexpr int LS = 4 * R + yz_pad<NL>();
+  constexpr int US = R + yz_upad<NL>();
   extern __shared__ float sw[];
   const int n = D == 1 ? P.ny : P.nz;
   float* const tab = sw;
   load_row_tables(tab, P.ctab[D], n, R);
-  float* const buf0 = sw + 6 * R;  // [8][LS]
-  // (the float offset 6 R + 8 LS = 38 R + 32 is even: 8-byte aligned)
-  double* const ubuf0 = reinterpret_cast<double*>(buf0 + WL_WARPS * LS);  // [8][R + 2]
+  float* const buf0 = sw + 6 * R;  // [NL][LS]
+  // (the float offset 6 R + NL LS = (6 + 4 NL) R + 32 is even: 8-byte aligned)
+  double* const ubuf0 = reinterpret_cast<double*>(buf0 + NL * LS);  // [NL][US]
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  const int c = threadIdx.x & 7, jc = threadIdx.x >> 3;  // this thread's share of a copy: line c, rows jc + 32 m
+  // this thread's share of a copy: line c, rows jc + 32 m
+  const int c = threadIdx.x & (NL - 1), jc = threadIdx.x / NL;
   const long long nl = nlines<D>(P);
-  const long long stride = (long long)gridDim.x * WL_WARPS;
+  const long long stride = (long long)gridDim.x * NL;
   const float* __restrict__ cib = P.cib[D];
   const float* __restrict__ cpp = P.cp[D];
   const float* __restrict__ cqq = P.cq[D];
@@ -740,7 +756,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
       cp.s32 = 32 * Lc.s;
     }
     float* const cr = buf0 + c * LS;
-    double* const cu = ubuf0 + c * (R + 2);
+    double* const cu = ubuf0 + c * US;
     if (cp.st) {
 #pragma unroll
       for (int m = 0; m < MX; m++) {
@@ -761,7 +777,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
     return cp;
   };
 
-  for (long long t0 = (long long)blockIdx.x * WL_WARPS; t0 < nl; t0 += stride) {
+  for (long long t0 = (long long)blockIdx.x * NL; t0 < nl; t0 += stride) {
     // a thread copies into exactly the rows it stored from last time: no
     // barrier needed before the copy
     const Copy cur = copy_in(t0);
@@ -783,7 +799,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_yzline32(const __grid_constan
     __syncthreads();
     if (cur.st) {
       const float* const cr = buf0 + c * LS;
-      const double* const cu = ubuf0 + c * (R + 2);
+      const double* const cu = ubuf0 + c * US;
 #pragma unroll
       for (int m = 0; m < MX; m++) {
         const int j = jc + 32 * m;
@@ -838,11 +854,13 @@ void launch_wline(const Dev& P, float* f, double* u, cudaStream_t st) {
   const bool acc = D == 2 && u;
   const size_t smem = acc ? yzline_smem<MX, true>() : yzline_smem<MX, false>();
   const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
-  const unsigned grid = (unsigned)std::min<long long>(need, (long long)P.sweep_blocks * per_sm);
+  const int nl_cta = acc ? yz_lines<true>() : yz_lines<false>();
+  const long long tiles = (nlines<D>(P) + nl_cta - 1) / nl_cta;
+  const unsigned grid = (unsigned)std::min<long long>(tiles, (long long)P.sweep_blocks * per_sm);
   if (acc)
-    k_yzline32<2, MX, true><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, u);
+    k_yzline32<2, MX, true><<<grid, 32 * nl_cta, smem, st>>>(P, f, u);
   else
-    k_yzline32<D == 0 ? 1 : D, MX, false><<<grid, 32 * WL_WARPS, smem, st>>>(P, f, nullptr);
+    k_yzline32<D == 0 ? 1 : D, MX, false><<<grid, 32 * nl_cta, smem, st>>>(P, f, nullptr);
 }
 
 template <int D>
