@@ -103,11 +103,9 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
   const int nx = P.nx, nrows = P.ny * P.nz;
   const long long sy = nx, sz = (long long)nx * P.ny;
   const double dt = P.dt;
-  // the y and z stencil weights of both sides in registers: a node's side
-  // selects one of two specialised bodies (uniform over a warp away from the
-  // interface) instead of indexing the weights per node
-  const double wy[2][3] = {{P.vd[1][0][0], P.vd[1][0][1], P.vd[1][0][2]}, {P.vd[1][1][0], P.vd[1][1][1], P.vd[1][1][2]}};
-  const double wz[2][3] = {{P.vd[2][0][0], P.vd[2][0][1], P.vd[2][0][2]}, {P.vd[2][1][0], P.vd[2][1][1], P.vd[2][1][2]}};
+  // a node's side selects one of two specialised bodies (uniform over a warp
+  // away from the interface), whose stencil weights are fixed kernel
+  // parameters (constant-bank operands) instead of weights indexed per node
   for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)nx * row;
@@ -151,14 +149,14 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
         auto node = [&](auto S) {
           constexpr int sd = decltype(S)::value;
           double sum = 0.0;
-          sum += uym[g] * wy[sd][0];
-          sum += uc[g] * wy[sd][1];
-          sum += uyp[g] * wy[sd][2];
+          sum += uym[g] * P.vd[1][sd][0];
+          sum += uc[g] * P.vd[1][sd][1];
+          sum += uyp[g] * P.vd[1][sd][2];
           const double ydt = dt * sum;
           sum = 0.0;
-          sum += uzm[g] * wz[sd][0];
-          sum += uc[g] * wz[sd][1];
-          sum += uzp[g] * wz[sd][2];
+          sum += uzm[g] * P.vd[2][sd][0];
+          sum += uc[g] * P.vd[2][sd][1];
+          sum += uzp[g] * P.vd[2][sd][2];
           const double zdt = dt * sum;
           const double src = row_source(P, q, ix, E, sd);
           double r = ydt + zdt;
@@ -173,7 +171,7 @@ __device__ __forceinline__ void k_adi_rhs_body(const Dev& P, unsigned cta_, unsi
 }
 
 template <int G>
-__global__ void __launch_bounds__(TPB) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
+__global__ void __launch_bounds__(TPB, 8) k_adi_rhs(const __grid_constant__ Dev P, const double* __restrict__ un,
                                                  double* __restrict__ R, double E) {
   k_adi_rhs_body<G>(P, blockIdx.x, gridDim.x, un, R, E);
 }

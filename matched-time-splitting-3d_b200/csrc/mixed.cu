@@ -29,22 +29,16 @@ namespace {
 // Residual rho = dt (A_x u + A_y u + A_z u + src), FP64 in, FP32 out.
 
 template <int G>
-__global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
+__global__ void __launch_bounds__(TPB, 8) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
                                                    float* __restrict__ rho, double E) {
   E = step_e(P, E, 2);
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
   const int nrows = P.ny * P.nz;
   const double dt = P.dt;
-  // stencil weights [dir][side][k] in registers; a node's side selects one
-  // of two specialised bodies (uniform over a warp away from the interface)
-  double wv[3][2][3];
-#pragma unroll
-  for (int d = 0; d < 3; d++)
-#pragma unroll
-    for (int sd = 0; sd < 2; sd++)
-#pragma unroll
-      for (int k = 0; k < 3; k++) wv[d][sd][k] = P.vd[d][sd][k];
+  // a node's side selects one of two specialised bodies (uniform over a
+  // warp away from the interface), whose stencil weights are fixed kernel
+  // parameters (constant-bank operands, no registers)
   for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)P.nx * row;
@@ -53,6 +47,15 @@ __global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P
       for (int ix = lane; ix < P.nx; ix += 32) rho[m0 + ix] = (float)(row_outer(P, q, ix, E) - un[m0 + ix]);
       continue;
     }
+    // the row and its four neighbour rows, indexed by ix (an interior row:
+    // uc_r[-1] and uc_r[nx] lie inside the field)
+    const double* const uc_r = un + m0;
+    const double* const uym_r = uc_r - sy;
+    const double* const uyp_r = uc_r + sy;
+    const double* const uzm_r = uc_r - sz;
+    const double* const uzp_r = uc_r + sz;
+    const uint8_t* const tg_r = P.tag + m0;
+    float* const rho_r = rho + m0;
     for (int ix0 = 0; ix0 < P.nx; ix0 += 32 * G) {
       double uc[G], uxm[G], uxp[G], uym[G], uyp[G], uzm[G], uzp[G];
       int tg[G];
@@ -60,39 +63,36 @@ __global__ void __launch_bounds__(TPB) k_adi_resid(const __grid_constant__ Dev P
       for (int g = 0; g < G; g++) {
         const int ix = ix0 + 32 * g + lane;
         if (ix < P.nx) {
-          // interior row: m0 - 1 and m0 + nx are inside the field
-          const long long m = m0 + ix;
-          tg[g] = P.tag[m];
-          uc[g] = un[m];
-          uxm[g] = un[m - 1];
-          uxp[g] = un[m + 1];
-          uym[g] = un[m - sy];
-          uyp[g] = un[m + sy];
-          uzm[g] = un[m - sz];
-          uzp[g] = un[m + sz];
+          tg[g] = tg_r[ix];
+          uc[g] = uc_r[ix];
+          uxm[g] = uc_r[ix - 1];
+          uxp[g] = uc_r[ix + 1];
+          uym[g] = uym_r[ix];
+          uyp[g] = uyp_r[ix];
+          uzm[g] = uzm_r[ix];
+          uzp[g] = uzp_r[ix];
         }
       }
 #pragma unroll
       for (int g = 0; g < G; g++) {
         const int ix = ix0 + 32 * g + lane;
         if (ix >= P.nx) break;
-        const long long m = m0 + ix;
         double r;
         if (ix == 0 || ix == P.nx - 1) {
           r = row_outer(P, q, ix, E) - uc[g];
         } else if (!(tg[g] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) {
           auto node = [&](auto S) {
             constexpr int sd = decltype(S)::value;
-            const double sx = (uxm[g] * wv[0][sd][0] + uc[g] * wv[0][sd][1]) + uxp[g] * wv[0][sd][2];
-            const double sy_ = (uym[g] * wv[1][sd][0] + uc[g] * wv[1][sd][1]) + uyp[g] * wv[1][sd][2];
-            const double sz_ = (uzm[g] * wv[2][sd][0] + uc[g] * wv[2][sd][1]) + uzp[g] * wv[2][sd][2];
+            const double sx = (uxm[g] * P.vd[0][sd][0] + uc[g] * P.vd[0][sd][1]) + uxp[g] * P.vd[0][sd][2];
+            const double sy_ = (uym[g] * P.vd[1][sd][0] + uc[g] * P.vd[1][sd][1]) + uyp[g] * P.vd[1][sd][2];
+            const double sz_ = (uzm[g] * P.vd[2][sd][0] + uc[g] * P.vd[2][sd][1]) + uzp[g] * P.vd[2][sd][2];
             return dt * (((sx + sy_) + sz_) + row_source(P, q, ix, E, sd));
           };
           r = (tg[g] & TAG_OUT) ? node(IntC<1>{}) : node(IntC<0>{});
         } else {
           continue;  // a MIB row: k_adi_resid_mib writes it
         }
-        rho[m] = (float)r;
+        rho_r[ix] = (float)r;
       }
     }
   }
