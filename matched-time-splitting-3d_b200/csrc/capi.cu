@@ -196,6 +196,18 @@ int line_count(const mts::Grid& g, int d) {
   return n1 * n2;
 }
 
+// Douglas-ADI steps of a single handle run their jumps and MIB
+// right-hand-side rows beside the pointwise pass, on a second stream that is
+// made when such a step is first launched (handles that only step in batches
+// never make one).
+cudaError_t ensure_side_stream(mts_problem* h) {
+  if (h->side.stream || h->prm.method != MTS_ADI) return cudaSuccess;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming);
+  return e;
+}
+
 // Builds every device-side table of a problem from its grid, tags and
 // crossing list, and uploads them.
 mts_status finish_create(mts_problem* h) {
@@ -495,13 +507,6 @@ mts_status finish_create(mts_problem* h) {
     for (int k = 0; k < 3; k++) D.shape[k] = def;
   }
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  if (p.method == MTS_ADI) {
-    // Douglas-ADI steps run their jumps and MIB right-hand-side rows beside
-    // the pointwise pass, on this second stream
-    CUDA_TRY(cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming));
-  }
   // row slack of the fields the sweeps stage whole chunks of: kRowPad rows of
   // the largest stride (an x-y plane)
   const size_t fpad = (size_t)mts::kRowPad * (size_t)g.nx * (size_t)g.ny;
@@ -649,6 +654,7 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
     h->ev_free.pop_back();
     ev = h->ev_busy.back().data();
   }
+  CUDA_TRY(ensure_side_stream(h));
   if (h->dev.precision == 1)
     h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev, &h->side);
   else
@@ -943,6 +949,7 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
     if (h->dev.precision != 1) continue;
+    BATCH_TRY(ensure_side_stream(h));
     for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
       h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
