@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <fstream>
+#include <iomanip>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -76,13 +77,18 @@ class GpuStepper {
   // TS::Solve_2nd(eq(t-dt), eq(t-dt/2), eq(t), inter, uh, beta)
   void Solve_2nd(Equation&, Equation&, Equation&, Intersections&, CubicDoub_I& uh, Beta&) { step(uh); }
 
-  // Douglas_ADI::Error: L-infinity with its argmax and L2 against the exact
-  // solution at the current time, written to the report stream.
+  // Douglas_ADI::Error (src/temporal/douglas_adi.cc:1723-1770): L-infinity
+  // with its argmax and L2 against the exact solution at the current time,
+  // written to the report stream in the reference's format.  The norms come
+  // from the device (mts_norms), bit-identical to the reference's loop.
   void Error(Equation&, CubicDoub_I&, std::ofstream& out) {
     double lmax, l2;
     int32_t am[3];
     check(mts_norms(h_, &lmax, &l2, am));
-    out << "L_inf = " << lmax << " at (" << am[0] << "," << am[1] << "," << am[2] << ")  L2 = " << l2 << "\n";
+    out << std::setprecision(3) << std::scientific;
+    out << "[Xmax,Ymax,Zmax] = [" << am[0] << "," << am[1] << "," << am[2] << "]" << std::endl;
+    out << " Lmax = " << lmax << ";  L2 = " << l2 << std::endl;
+    out << std::fixed << std::endl;
   }
 
   mts_handle handle() const { return h_; }

@@ -687,14 +687,15 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant
 // y and z lines: strided, so the CTA copies NL neighbouring lines together,
 // NL neighbours (4 NL bytes) of a row at a time, and warp w solves line w:
 // NL = 16 for y, 8 for z with the accumulation (whose FP64 state rows would
-// leave room for only one CTA of 16 per SM).  (A
+// leave room for only one CTA of 16 per SM).  (8 for the y lines of more than
+// 288 rows too, for more CTAs per SM, measured slower at 385^3.)  (A
 // second buffer, to copy the next 8 lines in while these are solved, was
 // measured slower: it halves the CTAs an SM holds, and they already overlap
 // one another's copies.)
 // ACC (z): the FP64 state is copied in with the right-hand side and the
 // increment is added to it instead of being stored, face lines included, so
 // that u^{n+1} = u^n + d at every node.
-template <bool ACC>
+template <bool ACC, int MX>
 __host__ __device__ constexpr int yz_lines() { return ACC ? 8 : 16; }
 // Padding of a line's rows so that a copy instruction's lanes (NL lines x
 // 32/NL rows) fall on distinct banks: 32/NL floats per line of (r, ib, p, q)
@@ -709,18 +710,18 @@ template <int MX, bool ACC>
 constexpr size_t yzline_smem() {
   // row tables 2 x 3 x R; NL lines x (r, ib, p, q: R each + padding); ACC:
   // NL lines x (R + padding) doubles
-  constexpr int NL = yz_lines<ACC>();
+  constexpr int NL = yz_lines<ACC, MX>();
   return sizeof(float) * ((size_t)6 * 32 * MX + (size_t)NL * (4 * 32 * MX + yz_pad<NL>())) +
          (ACC ? sizeof(double) * NL * (32 * MX + yz_upad<NL>()) : 0);
 }
 
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * yz_lines<ACC>()) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
+__global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
                                                           double* __restrict__ u) {
   static_assert(MX & 1, "odd rows per lane");
   static_assert(D != 0 && (!ACC || D == 2), "y and z lines; accumulation after the z solve");
   constexpr int R = 32 * MX;
-  constexpr int NL = yz_lines<ACC>();
+  constexpr int NL = yz_lines<ACC, MX>();
   constexpr int LS = 4 * R + yz_pad<NL>();
   constexpr int US = R + yz_upad<NL>();
   extern __shared__ float sw[];
@@ -854,7 +855,7 @@ void launch_wline(const Dev& P, float* f, double* u, cudaStream_t st) {
   const bool acc = D == 2 && u;
   const size_t smem = acc ? yzline_smem<MX, true>() : yzline_smem<MX, false>();
   const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, 232448 / (smem + 1024)));
-  const int nl_cta = acc ? yz_lines<true>() : yz_lines<false>();
+  const int nl_cta = acc ? yz_lines<true, MX>() : yz_lines<false, MX>();
   const long long tiles = (nlines<D>(P) + nl_cta - 1) / nl_cta;
   const unsigned grid = (unsigned)std::min<long long>(tiles, (long long)P.sweep_blocks * per_sm);
   if (acc)

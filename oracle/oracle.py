@@ -91,14 +91,15 @@ def reference_available(noaux: bool = False, dropin: bool = False) -> bool:
 
 
 def run_reference(prob: Problem, noaux: bool = False, timeout: float = 3600, dropin_gpu: bool = False,
-                  binary: str | None = None) -> RefResult:
+                  binary: str | None = None, report: str | None = None) -> RefResult:
     """Run the reference binary on ``prob``; raises RuntimeError when the
     reference aborts (it exits 0 on setup failures, so the JSON line is the
     success signal, as src/mesh/mesh.cc:64-65 and intersection.cc:2827 show).
 
     dropin_gpu: run the reference's setup and time loop with mts::GpuStepper
     stepping on the GPU in place of Douglas_ADI / LOD / TS (mts_dropin --gpu);
-    the setup is the noaux one.  binary: run this build instead."""
+    the setup is the noaux one.  binary: run this build instead.  report: a
+    path for the stepper's own Error() report after the last step."""
     binary = binary or (REF_BIN_DROPIN if dropin_gpu else REF_BIN_NOAUX if noaux else REF_BIN)
     with tempfile.TemporaryDirectory() as td:
         fu, fu0 = os.path.join(td, "u.bin"), os.path.join(td, "u0.bin")
@@ -106,6 +107,8 @@ def run_reference(prob: Problem, noaux: bool = False, timeout: float = 3600, dro
         cmd = [binary, *prob.ref_args(), "--dump-u", fu, "--dump-u0", fu0, "--dump-tags", ft, "--dump-mib", fm]
         if dropin_gpu:
             cmd.append("--gpu")
+        if report:
+            cmd += ["--report", report]
         cp = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         lines = [ln for ln in cp.stdout.splitlines() if ln.startswith("{")]
         if cp.returncode != 0 or not lines:

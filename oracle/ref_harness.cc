@@ -165,6 +165,7 @@ struct Args {
   int steps = -1;
   double t_end = 1.0;
   string dump_u, dump_tags, dump_mib, dump_u0;
+  string report;     // --report F: the stepper's own Error() text at the end
   bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
 };
 
@@ -174,7 +175,7 @@ struct Args {
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
           "        --beta bi bo --eq 0|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
-          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F]\n"
+          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F]\n"
 #ifdef MTS_DROPIN
           "        [--gpu]\n"
 #endif
@@ -237,6 +238,9 @@ Args parse(int argc, char** argv) {
     } else if (k == "--dump-mib") {
       need(1);
       a.dump_mib = argv[++i];
+    } else if (k == "--report") {
+      need(1);
+      a.report = argv[++i];
 #ifdef MTS_DROPIN
     } else if (k == "--gpu") {
       a.gpu = true;
@@ -415,6 +419,10 @@ int main(int argc, char** argv) {
       solve(st);
     }
     step_seconds = chrono::duration<double>(chrono::steady_clock::now() - s0).count();
+    if (!a.report.empty()) {
+      ofstream rep(a.report);
+      st.Error(*make_eq(a, t_now, beta), uh, rep);
+    }
   };
   auto adi_step = [&](auto& st) {
     auto eq = make_eq(a, t_now, beta);

@@ -60,11 +60,16 @@ def test_dropin_fails_loudly_without_a_device():
 @pytest.mark.gpu
 @needs_dropin
 @pytest.mark.parametrize("name,prob", CASES, ids=[c[0] for c in CASES])
-def test_dropin_gpu_equals_reference_bitwise(name, prob):
-    ref = O.run_reference(prob, noaux=True)
-    gpu = O.run_reference(prob, dropin_gpu=True)
+def test_dropin_gpu_equals_reference_bitwise(name, prob, tmp_path):
+    """Fields and norms bit for bit, and the stepper's Error() report (norms
+    from the device) the same text as the reference stepper's."""
+    ref = O.run_reference(prob, noaux=True, report=str(tmp_path / "ref.txt"))
+    gpu = O.run_reference(prob, dropin_gpu=True, report=str(tmp_path / "gpu.txt"))
     assert np.array_equal(gpu.u0, ref.u0), name
     diff = np.max(np.abs(gpu.u - ref.u))
     assert np.array_equal(gpu.u, ref.u), f"{name}: max |gpu - reference| = {diff}"
     for k in ("t", "lmax", "l2", "argmax", "ncross"):
         assert gpu.info[k] == ref.info[k], (name, k, gpu.info[k], ref.info[k])
+    ref_rep = (tmp_path / "ref.txt").read_text()
+    assert ref_rep.startswith("[Xmax,Ymax,Zmax] = [")
+    assert (tmp_path / "gpu.txt").read_text() == ref_rep
