@@ -2,9 +2,12 @@
 // that every floating-point operation rounds as in the reference build.
 #include "setup.h"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <thread>
 
 namespace mts {
 namespace {
@@ -615,9 +618,46 @@ Surface* make_surface(const mts_surface& s) {
   return nullptr;
 }
 
+namespace {
+
+// Host threads of a setup: one per 2^20 nodes, up to the cores (MTS_SETUP_THREADS
+// overrides), so that small problems, which servers set up many at a time on
+// their own pools, stay on one thread.
+int setup_threads(long long nodes) {
+  int t = (int)std::min<long long>(64, std::max<long long>(1, nodes >> 20));
+  const unsigned hw = std::thread::hardware_concurrency();
+  if (hw > 0) t = std::min(t, (int)hw);
+  if (const char* e = std::getenv("MTS_SETUP_THREADS")) {
+    const int v = std::atoi(e);
+    if (v > 0) t = v;
+  }
+  return t;
+}
+
+// Runs body(k) for k in [0, parts) on up to `threads` threads.
+template <class F>
+void run_parts(int parts, int threads, F body) {
+  threads = std::max(1, std::min(threads, parts));
+  if (threads == 1) {
+    for (int k = 0; k < parts; k++) body(k);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int w = 0; w < threads; w++)
+    pool.emplace_back([&, w] {
+      for (int k = w; k < parts; k += threads) body(k);
+    });
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
 mts_status build_tags(const Grid& g, const Surface& s, std::vector<int8_t>& tags) {
   tags.assign((size_t)g.nodes(), 0);
-  for (int iz = 0; iz < g.nz; iz++)
+  // planes in parallel; the first failing plane in order decides the status,
+  // as in one pass
+  std::vector<mts_status> st(g.nz, MTS_OK);
+  run_parts(g.nz, setup_threads(g.nodes()), [&](int iz) {
     for (int iy = 0; iy < g.ny; iy++)
       for (int ix = 0; ix < g.nx; ix++) {
         double v = s.set_node(g.x[ix], g.y[iy], g.z[iz]);
@@ -626,10 +666,15 @@ mts_status build_tags(const Grid& g, const Surface& s, std::vector<int8_t>& tags
           t = 1;
         else if (v < TOL_SETUP)
           t = -1;
-        else
-          return MTS_ERR_SETUP;  // "Interface on grid, reset the mesh!"
+        else {
+          st[iz] = MTS_ERR_SETUP;  // "Interface on grid, reset the mesh!"
+          return;
+        }
         tags[(size_t)g.index(ix, iy, iz)] = t;
       }
+  });
+  for (mts_status e : st)
+    if (e) return e;
   return MTS_OK;
 }
 
@@ -645,101 +690,144 @@ bool frame_inverse_col0(const double p[9], int row, double* out) {
   return true;
 }
 
+namespace {
+
+// The crossings of the d-lines with i1 in [i1a, i1b), in line order, into
+// out; the first failure stops the range and is returned.
+mts_status crossings_of_lines(const Grid& g, const std::vector<int8_t>& tags, const Surface& s, double beta_in,
+                              double beta_out, int mib, int d, int i1a, int i1b, std::vector<mts_crossing>& out,
+                              SetupReport& rep) {
+  const int n[3] = {g.nx, g.ny, g.nz};
+  const double h[3] = {g.dx, g.dy, g.dz};
+  const std::vector<double>* ax[3] = {&g.x, &g.y, &g.z};
+  // fixed axes of a d-line in the reference's (indx1, indx2) convention
+  const int a1 = d == 0 ? 1 : 0;
+  const int a2 = d == 2 ? 1 : 2;
+  for (int i1 = i1a; i1 < i1b; i1++)
+    for (int i2 = 1; i2 < n[a2] - 1; i2++) {
+      int idx3[3];
+      idx3[a1] = i1;
+      idx3[a2] = i2;
+      auto tag = [&](int j) {
+        idx3[d] = j;
+        return (double)tags[(size_t)g.index(idx3[0], idx3[1], idx3[2])];
+      };
+      auto point = [&](int j, double v, double c[3]) {
+        idx3[d] = j;
+        c[0] = g.x[idx3[0]];
+        c[1] = g.y[idx3[1]];
+        c[2] = g.z[idx3[2]];
+        c[d] = v;
+      };
+      // fixed coordinates for the root search along d
+      double fp = (*ax[a1])[i1], fq = (*ax[a2])[i2];
+      auto locate = [&](int j, Xing& q, int id) -> mts_status {
+        const std::vector<double>& v = *ax[d];
+        Root rt;
+        if (d == 0)
+          rt = gamma_root(s, 0, v[j], v[j + 1], fp, fq);
+        else if (d == 1)
+          rt = gamma_root(s, 1, v[j], v[j + 1], fp, fq);
+        else
+          rt = gamma_root(s, 2, v[j], v[j + 1], fp, fq);
+        if (!rt.ok) return MTS_ERR_NONFINITE;
+        std::memset(&q.c, 0, sizeof q.c);
+        q.c.dir = d;
+        q.c.indx1 = i1;
+        q.c.indx2 = i2;
+        q.c.id = id;
+        q.c.left_loc = j;
+        point(j, rt.value, q.c.coord);
+        q.c.gamma = q.c.coord[d] - v[j];
+        q.inside = beta_in;
+        q.outside = beta_out;
+        s.normal(q.c.coord[0], q.c.coord[1], q.c.coord[2], q.c.normal);
+        frame(d, q.c.normal, q.c.p);
+        return MTS_OK;
+      };
+      // Setup_Intersections scan (intersection.cc:79-291)
+      int ifp = 0;
+      int j = 1;
+      while (j < n[d] - 1) {
+        if (tag(j) * tag(j + 1) < 0) {
+          if (j + 2 >= n[d]) return MTS_ERR_SETUP;  // crossing in the last cell
+          if (tag(j + 1) * tag(j + 2) > 0) {
+            ifp += 1;
+            Xing q;
+            mts_status st = locate(j, q, ifp);
+            if (st) return st;
+            SolveResult r = mib == 1 ? irregular_l1(q, h[d]) : irregular_l2(q, h[d]);
+            if (!r.ok) return MTS_ERR_SETUP;
+            rep.singular_warnings += r.singular;
+            out.push_back(q.c);
+            j += 2;
+          } else {
+            if (j + 3 >= n[d] || tag(j + 2) * tag(j + 3) < 0) return MTS_ERR_SETUP;  // coherent corners
+            ifp += 1;
+            Xing l, r;
+            mts_status st = locate(j, l, -ifp);
+            if (st) return st;
+            ifp += 1;
+            st = locate(j + 1, r, -ifp);
+            if (st) return st;
+            SolveResult sr = mib == 1 ? corner_l1(l, r, h[d]) : corner_l2(l, r, h[d]);
+            if (!sr.ok) return MTS_ERR_SETUP;
+            rep.singular_warnings += sr.singular;
+            rep.corner_pairs += 1;
+            out.push_back(l.c);
+            out.push_back(r.c);
+            j += 3;
+          }
+        } else {
+          j += 1;
+        }
+      }
+      if (ifp % 2 == 1) return MTS_ERR_SETUP;  // open surface
+    }
+  return MTS_OK;
+}
+
+}  // namespace
+
 mts_status build_crossings(const Grid& g, const std::vector<int8_t>& tags, const Surface& s,
                            double beta_in, double beta_out, int mib,
                            std::vector<mts_crossing>& out, SetupReport* report) {
   out.clear();
-  SetupReport rep;
-  const int n[3] = {g.nx, g.ny, g.nz};
-  const double h[3] = {g.dx, g.dy, g.dz};
-  const std::vector<double>* ax[3] = {&g.x, &g.y, &g.z};
   if (mib != 1 && mib != 2) return MTS_ERR_ARG;
-
+  const int n[3] = {g.nx, g.ny, g.nz};
+  // Every line's crossings and weights depend on that line alone: ranges of
+  // lines run on their own threads into their own lists, which are joined in
+  // line order (direction, i1, i2), the order of one pass.  The first failing
+  // range in that order decides the status, as in one pass.
+  struct Range {
+    int d, a, b;
+    std::vector<mts_crossing> out;
+    SetupReport rep;
+    mts_status st = MTS_OK;
+  };
+  std::vector<Range> ranges;
+  const int threads = setup_threads(g.nodes());
   for (int d = 0; d < 3; d++) {
-    // fixed axes of a d-line in the reference's (indx1, indx2) convention
-    int a1 = d == 0 ? 1 : 0;
-    int a2 = d == 2 ? 1 : 2;
-    for (int i1 = 1; i1 < n[a1] - 1; i1++)
-      for (int i2 = 1; i2 < n[a2] - 1; i2++) {
-        int idx3[3];
-        idx3[a1] = i1;
-        idx3[a2] = i2;
-        auto tag = [&](int j) {
-          idx3[d] = j;
-          return (double)tags[(size_t)g.index(idx3[0], idx3[1], idx3[2])];
-        };
-        auto point = [&](int j, double v, double c[3]) {
-          idx3[d] = j;
-          c[0] = g.x[idx3[0]];
-          c[1] = g.y[idx3[1]];
-          c[2] = g.z[idx3[2]];
-          c[d] = v;
-        };
-        // fixed coordinates for the root search along d
-        double fp = (*ax[a1])[i1], fq = (*ax[a2])[i2];
-        auto locate = [&](int j, Xing& q, int id) -> mts_status {
-          const std::vector<double>& v = *ax[d];
-          Root rt;
-          if (d == 0)
-            rt = gamma_root(s, 0, v[j], v[j + 1], fp, fq);
-          else if (d == 1)
-            rt = gamma_root(s, 1, v[j], v[j + 1], fp, fq);
-          else
-            rt = gamma_root(s, 2, v[j], v[j + 1], fp, fq);
-          if (!rt.ok) return MTS_ERR_NONFINITE;
-          std::memset(&q.c, 0, sizeof q.c);
-          q.c.dir = d;
-          q.c.indx1 = i1;
-          q.c.indx2 = i2;
-          q.c.id = id;
-          q.c.left_loc = j;
-          point(j, rt.value, q.c.coord);
-          q.c.gamma = q.c.coord[d] - v[j];
-          q.inside = beta_in;
-          q.outside = beta_out;
-          s.normal(q.c.coord[0], q.c.coord[1], q.c.coord[2], q.c.normal);
-          frame(d, q.c.normal, q.c.p);
-          return MTS_OK;
-        };
-        // Setup_Intersections scan (intersection.cc:79-291)
-        int ifp = 0;
-        int j = 1;
-        while (j < n[d] - 1) {
-          if (tag(j) * tag(j + 1) < 0) {
-            if (j + 2 >= n[d]) return MTS_ERR_SETUP;  // crossing in the last cell
-            if (tag(j + 1) * tag(j + 2) > 0) {
-              ifp += 1;
-              Xing q;
-              mts_status st = locate(j, q, ifp);
-              if (st) return st;
-              SolveResult r = mib == 1 ? irregular_l1(q, h[d]) : irregular_l2(q, h[d]);
-              if (!r.ok) return MTS_ERR_SETUP;
-              rep.singular_warnings += r.singular;
-              out.push_back(q.c);
-              j += 2;
-            } else {
-              if (j + 3 >= n[d] || tag(j + 2) * tag(j + 3) < 0) return MTS_ERR_SETUP;  // coherent corners
-              ifp += 1;
-              Xing l, r;
-              mts_status st = locate(j, l, -ifp);
-              if (st) return st;
-              ifp += 1;
-              st = locate(j + 1, r, -ifp);
-              if (st) return st;
-              SolveResult sr = mib == 1 ? corner_l1(l, r, h[d]) : corner_l2(l, r, h[d]);
-              if (!sr.ok) return MTS_ERR_SETUP;
-              rep.singular_warnings += sr.singular;
-              rep.corner_pairs += 1;
-              out.push_back(l.c);
-              out.push_back(r.c);
-              j += 3;
-            }
-          } else {
-            j += 1;
-          }
-        }
-        if (ifp % 2 == 1) return MTS_ERR_SETUP;  // open surface
-      }
+    const int a1 = d == 0 ? 1 : 0;
+    const int lo = 1, hi = n[a1] - 1;
+    const int per = std::max(1, (hi - lo + 4 * threads - 1) / (4 * threads));
+    for (int a = lo; a < hi; a += per) ranges.push_back(Range{d, a, std::min(hi, a + per), {}, {}, MTS_OK});
+  }
+  run_parts((int)ranges.size(), threads, [&](int k) {
+    Range& r = ranges[k];
+    r.st = crossings_of_lines(g, tags, s, beta_in, beta_out, mib, r.d, r.a, r.b, r.out, r.rep);
+  });
+  SetupReport rep;
+  size_t total = 0;
+  for (const Range& r : ranges) {
+    if (r.st) return r.st;
+    total += r.out.size();
+  }
+  out.reserve(total);
+  for (const Range& r : ranges) {
+    out.insert(out.end(), r.out.begin(), r.out.end());
+    rep.singular_warnings += r.rep.singular_warnings;
+    rep.corner_pairs += r.rep.corner_pairs;
   }
   if (report) *report = rep;
   return MTS_OK;

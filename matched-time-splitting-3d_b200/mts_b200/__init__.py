@@ -76,9 +76,10 @@ def setup_host(spec: Spec):
 
 
 def batch_advance(solvers, nsteps: int) -> None:
-    """nsteps steps of every solver in one batch (mts_batch_advance): one CUDA
-    graph holding a step of each problem, replayed.  Results equal those of
-    advancing each solver on its own."""
+    """nsteps steps of every solver in one batch (mts_batch_advance): each
+    kernel of a step is one launch for all plain-form problems of a method,
+    a CTA working on one problem's part.  Results equal those of advancing
+    each solver on its own."""
     solvers = list(solvers)
     if not solvers:
         return
