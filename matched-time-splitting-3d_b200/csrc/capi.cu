@@ -325,10 +325,10 @@ mts_status finish_create(mts_problem* h) {
   }
   // Thomas factorisation (the factor half of TDMA, douglas_adi.cc:1790-1798:
   // gam_j = c_{j-1}/bet, bet = b_j - a_j*gam_j, same operations): prefix
-  // tables per direction and row-1 side, and per-node factors from the first
-  // MIB row on for the lines that cross the interface.
+  // tables per direction and row-1 side here; the per-node factors of the
+  // lines that cross the interface, from their first MIB row on, are
+  // computed on the device once the tables are there (launch_factor_lines).
   std::vector<double> ptab[3][2];
-  std::vector<double> fbet[3], fgam[3];
   {
     const int n[3] = {g.nx, g.ny, g.nz};
     std::vector<double> a, b, c;
@@ -368,49 +368,6 @@ mts_status finish_create(mts_problem* h) {
         for (int j = 0; j < len; j++) {
           ptab[d][side][2 * j] = lb[j];
           ptab[d][side][2 * j + 1] = lg[j];
-        }
-      }
-      if (blocks[d].empty()) continue;
-      fbet[d].assign((size_t)N, 0.0);
-      fgam[d].assign((size_t)N, 0.0);
-      const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
-      const int n2 = n[a2];
-      for (size_t k = 0; k < blocks[d].size();) {
-        const int line = blocks[d][k].line;
-        const int i1 = line / n2, i2 = line % n2;
-        int idx3[3];
-        idx3[a1] = i1;
-        idx3[a2] = i2;
-        auto node = [&](int j) {
-          idx3[d] = j;
-          return g.index(idx3[0], idx3[1], idx3[2]);
-        };
-        a[0] = 0.0;
-        b[0] = 1.0;
-        c[0] = 0.0;
-        for (int j = 1; j < len - 1; j++) {
-          int side = h->tags[(size_t)node(j)] == 1;
-          a[j] = D.ia[d][side];
-          b[j] = D.ib[d][side];
-          c[j] = D.ic[d][side];
-        }
-        a[len - 1] = 0.0;
-        b[len - 1] = 1.0;
-        c[len - 1] = 0.0;
-        const int L1 = blocks[d][k].L;
-        for (; k < blocks[d].size() && blocks[d][k].line == line; k++) {
-          const mts::MibBlock& bk = blocks[d][k];
-          for (int q = 0; q < bk.kind; q++) {
-            a[bk.L + q] = bk.ia[q];
-            b[bk.L + q] = bk.ib[q];
-            c[bk.L + q] = bk.ic[q];
-          }
-        }
-        if (!factor(len, lb, lg)) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line factorisation");
-        for (int j = L1; j < len; j++) {
-          long long m = node(j);
-          fbet[d][(size_t)m] = lb[j];
-          fgam[d][(size_t)m] = lg[j];
         }
       }
     }
@@ -525,13 +482,20 @@ mts_status finish_create(mts_problem* h) {
     CUDA_TRY(h->put(&rbk, (const double*)nullptr, 3 * blocks[d].size()));
     D.rblk[d] = rbk;
     D.nblk[d] = (int)blocks[d].size();
+    // per-node factor fields of the crossing lines (zero elsewhere), FP64
+    // and, for the mixed form, FP32 (1/bet and gam): filled on the device
     double *fb = nullptr, *fg = nullptr;
-    if (!fbet[d].empty()) {
-      CUDA_TRY(h->put_padded(&fb, fbet[d].data(), fbet[d].size(), fpad));
-      CUDA_TRY(h->put_padded(&fg, fgam[d].data(), fgam[d].size(), fpad));
+    float *fb32 = nullptr, *fg32 = nullptr;
+    if (!blocks[d].empty()) {
+      CUDA_TRY(h->put_padded(&fb, (const double*)nullptr, (size_t)N, fpad));
+      CUDA_TRY(h->put_padded(&fg, (const double*)nullptr, (size_t)N, fpad));
+      CUDA_TRY(h->put_padded(&fb32, (const float*)nullptr, (size_t)N, fpad));
+      CUDA_TRY(h->put_padded(&fg32, (const float*)nullptr, (size_t)N, fpad));
     }
     D.fbet[d] = fb;
     D.fgam[d] = fg;
+    D.fib32[d] = fb32;
+    D.fgam32[d] = fg32;
     // the same factors in FP32 for the mixed-precision sweeps, as 1/bet and gam
     for (int side = 0; side < 2; side++) {
       std::vector<float> p32(ptab[d][side].size());
@@ -543,18 +507,6 @@ mts_status finish_create(mts_problem* h) {
       CUDA_TRY(h->put(&pt, p32.data(), p32.size()));
       D.ptab32[d][side] = pt;
     }
-    float *fb32 = nullptr, *fg32 = nullptr;
-    if (!fbet[d].empty()) {
-      std::vector<float> v((size_t)N);
-      for (size_t m = 0; m < v.size(); m++) v[m] = fbet[d][m] != 0.0 ? (float)(1.0 / fbet[d][m]) : 0.0f;
-      CUDA_TRY(h->put_padded(&fb32, v.data(), v.size(), fpad));
-      for (size_t m = 0; m < v.size(); m++) v[m] = (float)fgam[d][m];
-      CUDA_TRY(h->put_padded(&fg32, v.data(), v.size(), fpad));
-      // the host copies must outlive the asynchronous uploads
-      CUDA_TRY(cudaStreamSynchronize(h->stream));
-    }
-    D.fib32[d] = fb32;
-    D.fgam32[d] = fg32;
     float* rb32 = nullptr;
     CUDA_TRY(h->put(&rb32, (const float*)nullptr, 3 * blocks[d].size()));
     D.rblk32[d] = rb32;
@@ -606,6 +558,16 @@ mts_status finish_create(mts_problem* h) {
   CUDA_TRY(h->put(&D.jv, (const double2*)nullptr, h->cross.size()));
   CUDA_TRY(h->put(&D.status, (const int*)nullptr, 1));
   CUDA_TRY(cudaMemsetAsync(D.status, 0, sizeof(int), h->stream));
+  {
+    // the crossing lines' per-node factors; a zero pivot raises D.status
+    mts::launch_factor_lines(D, D.status, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    int zero_pivot = 0;
+    CUDA_TRY(cudaMemcpyAsync(&zero_pivot, D.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (zero_pivot) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line factorisation");
+    CUDA_TRY(cudaMemsetAsync(D.status, 0, sizeof(int), h->stream));
+  }
   h->norm_nb = mts::norms_blocks(D);
   CUDA_TRY(h->put(&h->norm_part, (const double*)nullptr, (size_t)3 * h->norm_nb));
   CUDA_TRY(h->put(&h->norm_out, (const double*)nullptr, 3));

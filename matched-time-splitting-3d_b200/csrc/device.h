@@ -149,6 +149,9 @@ struct StepTimes {
 // Host-side launchers (kernels.cu).  All enqueue on `stream` and return the
 // number of kernel launches made.
 int launch_initialize(const Dev& P, double E, double* u, cudaStream_t stream);
+// Per-node Thomas factors of the lines with MIB blocks (once, at setup);
+// *zero_pivot is set on a zero pivot.
+int launch_factor_lines(const Dev& P, int* zero_pivot, cudaStream_t stream);
 // ev: null, or 2 events per kernel slot recorded around each launch.
 // A second stream with its fork and join events (timing off), for work of a
 // step that can run beside the main stream's.

@@ -844,6 +844,65 @@ __global__ void __launch_bounds__(NT, 1) k_sweep(const __grid_constant__ Dev P, 
   k_sweep_body<D, KIND, CH, NS, NT>(P, blockIdx.x, gridDim.x, io);
 }
 
+// Thomas factors of the lines that cross the interface (the factor half of
+// TDMA, douglas_adi.cc:1790-1798: gam_j = c_{j-1}/bet, bet = b_j - a_j*gam_j,
+// the same IEEE operations as the host's prefix tables), once at setup, one
+// thread per line.  A line's rows are the identity on its faces, the regular
+// three-point rows of the node's side elsewhere, and the Convert2Tri rows of
+// its blocks; from the first MIB row on, bet and gam are stored per node in
+// FP64 (fbet, fgam) and as 1/bet and gam in FP32 (fib32, fgam32).  A zero
+// pivot sets *zero_pivot.
+template <int D>
+__global__ void __launch_bounds__(TPB) k_factor_lines(const __grid_constant__ Dev P, int* zero_pivot) {
+  const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (t >= nlines<D>(P)) return;
+  Line L;
+  decode_line<D>(P, t, L);
+  if (L.boundary) return;
+  const int bfirst = P.bstart[D][L.lid], bend = P.bstart[D][L.lid + 1];
+  if (bfirst == bend) return;
+  const MibBlock* const blk = P.blk[D];
+  const int n = L.n;
+  const int L1 = blk[bfirst].L;
+  int b = bfirst;
+  double bet = 1.0;   // row 0: b = 1
+  double cprev = 0.0; // c of the previous row
+  for (int j = 1; j < n; j++) {
+    double aj, bj, cj;
+    if (j == n - 1) {
+      aj = 0.0;
+      bj = 1.0;
+      cj = 0.0;
+    } else if (b < bend && j >= blk[b].L) {
+      const int q = j - blk[b].L;
+      aj = blk[b].ia[q];
+      bj = blk[b].ib[q];
+      cj = blk[b].ic[q];
+      if (q == blk[b].kind - 1) b++;
+    } else {
+      const int side = (P.tag[L.base + (long long)j * L.s] & TAG_OUT) ? 1 : 0;
+      aj = P.ia[D][side];
+      bj = P.ib[D][side];
+      cj = P.ic[D][side];
+    }
+    const double gm = cprev / bet;
+    bet = bj - aj * gm;
+    if (bet == 0.0) {
+      atomicOr(zero_pivot, 1);
+      return;
+    }
+    if (j >= L1) {
+      // (the factor fields are read-only to the step kernels; setup fills them here)
+      const long long m = L.base + (long long)j * L.s;
+      const_cast<double*>(P.fbet[D])[m] = bet;
+      const_cast<double*>(P.fgam[D])[m] = gm;
+      const_cast<float*>(P.fib32[D])[m] = (float)(1.0 / bet);
+      const_cast<float*>(P.fgam32[D])[m] = (float)gm;
+    }
+    cprev = cj;
+  }
+}
+
 // Refresh_Jump (intersection.cc:2294-2490): [u] and u_dir per crossing.
 __device__ __forceinline__ void k_jumps_body(const Dev& P, unsigned cta_, unsigned ncta_, double E) {
   int c = cta_ * TPB + threadIdx.x;
@@ -1021,6 +1080,23 @@ void launch_jumps(const Dev& P, double E, cudaStream_t st) {
 }
 
 unsigned pointwise_rows_grid(const Dev& P) { return pointwise_blocks(P); }
+
+int launch_factor_lines(const Dev& P, int* zero_pivot, cudaStream_t st) {
+  int launches = 0;
+  if (P.nblk[0] > 0) {
+    k_factor_lines<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, zero_pivot);
+    launches++;
+  }
+  if (P.nblk[1] > 0) {
+    k_factor_lines<1><<<(unsigned)((nlines<1>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, zero_pivot);
+    launches++;
+  }
+  if (P.nblk[2] > 0) {
+    k_factor_lines<2><<<(unsigned)((nlines<2>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, zero_pivot);
+    launches++;
+  }
+  return launches;
+}
 
 int launch_initialize(const Dev& P, double E, double* u, cudaStream_t st) {
   k_init<<<pointwise_blocks(P), TPB, 0, st>>>(P, E, u);
