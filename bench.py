@@ -241,6 +241,7 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
             "p99_s": float(np.percentile(lat, 99)), "sequential_p50_s": float(np.percentile(seq_lat, 50)),
             "sequential_p99_s": float(np.percentile(seq_lat, 99)), "peak_active": srv.peak_active,
             "peak_budget_bytes": srv.peak_bytes, "batches": srv.batches,
+            "loop_batch_s": srv.batch_s, "loop_retire_s": srv.retire_s,
             "solves_per_s_vs_sequential": len(res) / span / out["sequential_solves_per_s"],
         }
     out["timing"] = ("wall clock from the first arrival to the last completion; latency = completion - arrival; "

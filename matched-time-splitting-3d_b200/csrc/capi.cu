@@ -851,11 +851,23 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
       hs[i]->dev.tstop = counts[i];
     }
   }
+  // Problems whose lines fill the GPU by themselves (256 per SM or more in
+  // every direction), and mixed-precision ones, step on their own streams
+  // with their own launch shapes (in a batched launch a large grid would run
+  // with the small shared-SM shape); the rest are batched per method.  Every
+  // group and every solo problem is on its own stream, so they all run at
+  // once; the results are those of stepping each problem alone either way.
+  auto fills_gpu = [&](const mts_problem* h) {
+    long long lines = line_count(h->g, 0);
+    for (int d = 1; d < 3; d++) lines = std::min(lines, (long long)line_count(h->g, d));
+    return lines >= 256LL * h->dev.sweep_blocks;
+  };
+  auto solo = [&](int i) { return hs[i]->dev.precision != 0 || fills_gpu(hs[i]); };
   // plain handles by method: one batched launch sequence per group
   for (int method = 0; method < 4; method++) {
     std::vector<int> mem;
     for (int i = 0; i < n; i++)
-      if (hs[i]->dev.precision == 0 && hs[i]->prm.method == method) mem.push_back(i);
+      if (!solo(i) && hs[i]->prm.method == method) mem.push_back(i);
     if (mem.empty()) continue;
     cudaStream_t q = nullptr;
     BATCH_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
@@ -905,24 +917,27 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     for (int k = 0; k < gsteps; k++) launches += mts::launch_step_batch(plan, q);
     BATCH_TRY(cudaGetLastError());
     for (int i : mem) hs[i]->launches += launches;
-    BATCH_TRY(cudaStreamSynchronize(q));
   }
-  // mixed-precision handles: their own steps on their own streams
+  // solo problems: their own steps on their own streams
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
-    if (h->dev.precision != 1) continue;
+    if (!solo(i)) continue;
     BATCH_TRY(ensure_side_stream(h));
     for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
-      h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
+      if (h->dev.precision == 1)
+        h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
+      else
+        h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, nullptr, &h->side);
       mts::launch_tick(h->dev, h->stream);
       h->launches++;
     }
     BATCH_TRY(cudaGetLastError());
   }
+  for (cudaStream_t q : streams) BATCH_TRY(cudaStreamSynchronize(q));
   for (int i = 0; i < n; i++) {
     mts_problem* h = hs[i];
-    if (h->dev.precision == 1) {
+    if (solo(i)) {
       mts_status s2 = sync_status(h);
       if (s2 && !st) st = s2;
     }

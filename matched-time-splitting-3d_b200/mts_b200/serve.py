@@ -11,8 +11,9 @@ Each goes through
      up to chunk_steps steps; one launch per kernel of a step for all of
      them), so problems that arrive while others run join the batch as soon
      as they are uploaded, and their work overlaps on the device,
-  4. retirement: after its last step a problem's error norms are read, its
-     device memory is freed and its budget returned.
+  4. retirement: after its last step a pool thread reads the problem's
+     error norms and frees its device memory; its budget is returned when
+     that is done.  The loop goes on batching meanwhile.
 Batching does not change any result: each problem's solution is the one it
 gets alone, bit for bit (mts_batch_advance_steps' contract).
 """
@@ -76,12 +77,27 @@ class Server:
         self.peak_bytes = 0
         self.peak_active = 0
         self.batches = 0
+        # seconds of the loop in batch calls and in retirements (norms, field
+        # read, free), for the breakdown of a run
+        self.batch_s = 0.0
+        self.retire_s = 0.0
 
     # -- pool tasks ----------------------------------------------------------
     def _setup(self, job: _Job) -> _Job:
         tags, cr, _ = setup_host(job.req.spec)
         job.tags, job.crossings = tags, cr
         job.bound = device_bytes_bound(job.req.spec, len(cr), precision=self.precision)
+        return job
+
+    def _retire(self, job: _Job, clock) -> _Job:
+        res = job.result
+        lmax, l2, _ = job.solver.norms()
+        res.lmax, res.l2, res.t, res.steps = lmax, l2, job.solver.time, job.req.steps
+        if self.keep:
+            res.solution = job.solver.solution()
+        job.solver.close()
+        job.solver = None
+        res.done = clock()
         return job
 
     def _upload(self, job: _Job) -> _Job:
@@ -100,7 +116,7 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.arrival)
         results = {r.id: Result(r.id, r.arrival) for r in reqs}
         pool = ThreadPoolExecutor(max_workers=self.threads)
-        setups, uploads = [], []          # futures in flight
+        setups, uploads, retires = [], [], []  # futures in flight
         ready: list[_Job] = []            # set up, waiting for budget
         active: list[_Job] = []           # on the device
         used = 0
@@ -108,7 +124,7 @@ class Server:
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0  # noqa: E731
         try:
-            while nxt < len(reqs) or setups or ready or uploads or active:
+            while nxt < len(reqs) or setups or ready or uploads or active or retires:
                 now = clock()
                 # 1. arrivals -> host setup
                 while nxt < len(reqs) and reqs[nxt].arrival <= now:
@@ -126,7 +142,11 @@ class Server:
                     job = ready.pop(0)
                     used += job.bound
                     uploads.append(pool.submit(self._upload, job))
-                if ready and not active and not uploads and ready[0].bound > self.budget:
+                # finished retirements return their budget
+                for f in [f for f in retires if f.done()]:
+                    retires.remove(f)
+                    used -= f.result().bound
+                if ready and not active and not uploads and not retires and ready[0].bound > self.budget:
                     raise RuntimeError(f"request {ready[0].req.id} needs {ready[0].bound} bytes, over the budget")
                 done_u = [f for f in uploads if f.done()]
                 for f in done_u:
@@ -139,26 +159,23 @@ class Server:
                 # 4. one chunk of the running batch
                 if active:
                     ks = [min(self.chunk, j.left) for j in active]
+                    tb = time.perf_counter()
                     batch_advance_steps([j.solver for j in active], ks)
+                    self.batch_s += time.perf_counter() - tb
                     self.batches += 1
                     for j, k in zip(active, ks):
                         j.left -= k
+                    tr = time.perf_counter()
                     for j in [j for j in active if j.left == 0]:
-                        lmax, l2, _ = j.solver.norms()
-                        res = j.result
-                        res.lmax, res.l2, res.t, res.steps = lmax, l2, j.solver.time, j.req.steps
-                        if self.keep:
-                            res.solution = j.solver.solution()
-                        j.solver.close()
-                        used -= j.bound
-                        res.done = clock()
                         active.remove(j)
+                        retires.append(pool.submit(self._retire, j, clock))
+                    self.retire_s += time.perf_counter() - tr
                 else:
                     time.sleep(0.0005)
         finally:
+            pool.shutdown(wait=True)
             for j in active:
                 j.solver.close()
-            pool.shutdown(wait=True)
         return [results[r.id] for r in reqs]
 
 

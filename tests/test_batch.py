@@ -1,5 +1,7 @@
-"""Batched stepping (mts_batch_advance): one CUDA graph holding a step of
-every problem, replayed.  Each problem's result must be bit-identical to
+"""Batched stepping (mts_batch_advance): the plain problems of a method
+advance together, one launch per kernel of a step for all of them; large and
+mixed-precision problems step on their own streams alongside.  Each
+problem's result must be bit-identical to
 stepping it alone, whatever the mix of methods, MIB variants, grid shapes,
 beta ratios and precision forms in the batch (the problems are drawn as the
 batched workload draws them: anisotropic grids, shifted ellipsoids, beta_out
@@ -50,7 +52,7 @@ def test_batch_equals_individual_runs():
         for s, p in zip(solvers, precision):
             s.set_precision(p)
             s.initialize()
-        M.batch_advance(solvers, 5)   # odd: the two-step graph plus one step outside it
+        M.batch_advance(solvers, 5)
         M.batch_advance(solvers, 4)
         for sp, s, p in zip(specs, solvers, precision):
             u, t = solve_alone(sp, p, 9)
@@ -75,6 +77,33 @@ def test_batch_with_per_problem_step_counts():
     rng = np.random.default_rng(21)
     specs = [draw(rng) for _ in range(8)]
     counts = [int(c) for c in rng.integers(0, 7, len(specs))]
+    solvers = [M.Solver(sp) for sp in specs]
+    try:
+        for s in solvers:
+            s.initialize()
+        M.batch_advance_steps(solvers, counts)
+        for sp, s, c in zip(specs, solvers, counts):
+            u, t = solve_alone(sp, "plain", c)
+            assert s.time == t
+            assert np.array_equal(s.solution(), u), (sp, c)
+    finally:
+        for s in solvers:
+            s.close()
+
+
+def test_batch_with_large_problems_on_their_own_streams():
+    """Problems whose lines fill the GPU (here 200^3 = 39,204 lines a
+    direction, plain ADI and TS) step on their own streams with their own
+    shapes, beside the batched small ones and a 129^3 one: every result is
+    still that of stepping the problem alone."""
+    rng = np.random.default_rng(5)
+    specs = [draw(rng) for _ in range(3)]
+    specs.append(M.Spec(n=(129, 129, 129), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0,
+                        beta_out=1000.0, method="lod-cn", mib=1, dt=2.0 / 128))
+    for method in ("adi", "ts"):
+        specs.append(M.Spec(n=(200, 200, 200), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0,
+                            beta_out=1000.0, method=method, mib=2, dt=2.0 / 199))
+    counts = [3, 0, 5, 2, 4, 3]
     solvers = [M.Solver(sp) for sp in specs]
     try:
         for s in solvers:
