@@ -63,13 +63,17 @@ class Server:
     """Continuous-batching server over the C ABI.
 
     hbm_budget: bytes of device memory the admitted problems may hold.
+    max_active: problems on the device at once (admitted and not retired); a
+      batch call's cost grows faster than its problem count, so past a few
+      hundred problems more of them in flight lower the throughput.
     chunk_steps: steps per batch call; new arrivals join at chunk boundaries.
     host_threads: pool for host setup and uploads.
     keep_solutions: keep each result's final field (for tests)."""
 
     def __init__(self, hbm_budget: float = 120e9, chunk_steps: int = 8, host_threads: int = 16,
-                 keep_solutions: bool = False, precision: str = "plain"):
+                 keep_solutions: bool = False, precision: str = "plain", max_active: int = 256):
         self.budget = int(hbm_budget)
+        self.max_active = max(1, int(max_active))
         self.chunk = max(1, int(chunk_steps))
         self.threads = max(1, int(host_threads))
         self.keep = keep_solutions
@@ -137,8 +141,10 @@ class Server:
                     setups.remove(f)
                     ready.append(f.result())
                 ready.sort(key=lambda j: j.req.arrival)
-                # 3. admission against the budget (first come, first served)
-                while ready and used + ready[0].bound <= self.budget:
+                # 3. admission against the budget and the active cap (first
+                # come, first served)
+                while (ready and used + ready[0].bound <= self.budget
+                       and len(active) + len(uploads) < self.max_active):
                     job = ready.pop(0)
                     used += job.bound
                     uploads.append(pool.submit(self._upload, job))

@@ -98,3 +98,12 @@ def test_fifo_latencies():
     a = np.array([0.0, 0.5, 0.6, 5.0])
     s = np.array([1.0, 1.0, 1.0, 1.0])
     assert np.allclose(serve.fifo_latencies(a, s), [1.0, 1.5, 2.4, 1.0])
+
+
+def test_active_cap_bounds_problems_in_flight(fakes):
+    """max_active bounds the problems on the device at once; every request
+    still completes."""
+    srv = serve.Server(hbm_budget=1e9, chunk_steps=2, host_threads=4, max_active=3)
+    out = srv.run(reqs(30, 0.0))
+    assert [r.id for r in out] == list(range(30))
+    assert 1 <= srv.peak_active <= 3
