@@ -234,8 +234,10 @@ mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
  * of douglas_adi.cc:66-1110 run on the FP32 increment with FP32 factors, and
  * the increment is added to the FP64 state.  Results differ from the plain
  * form by the FP32 rounding of one step's increment per step; the error
- * against the exact solution stays that of the plain form.  No counterpart
- * in the reference, which computes in FP64 only. */
+ * against the exact solution stays that of the plain form.  Switching the
+ * form on builds its per-node FP32 coefficients on the device once (3 x 4
+ * bytes per node and direction, for lines of up to 544 rows).  No
+ * counterpart in the reference, which computes in FP64 only. */
 typedef enum { MTS_PRECISION_PLAIN = 0, MTS_PRECISION_MIXED = 1 } mts_precision;
 mts_status mts_set_precision(mts_handle h, int32_t precision);
 mts_status mts_get_precision(mts_handle h, int32_t* precision);
