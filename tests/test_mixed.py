@@ -77,6 +77,33 @@ def test_mixed_segment_edges(n):
     assert l_m <= LINF_RATIO * l_p
 
 
+@pytest.mark.parametrize("n", [(400, 33, 35), (33, 520, 35), (35, 33, 300)])
+def test_mixed_long_lines_within_the_segments(n):
+    """Lines of 289-544 rows (13 and 17 rows per lane) in x, in y, and in z
+    with the accumulation; dt = the finest spacing."""
+    spec = M.Spec(n=n, surface="ellipsoid", surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
+                  beta_in=1.0, beta_out=100.0, method="adi", mib=2, dt=2.0 / (max(n) - 1))
+    u_p, (l_p, _, _) = run(spec, "plain", 4)
+    u_m, (l_m, _, _) = run(spec, "mixed", 4)
+    assert rel_maxdiff(u_m, u_p) <= REL_TOL
+    assert l_m <= LINF_RATIO * l_p
+
+
+def test_mixed_stiff_long_lines():
+    """400-row x lines with dt set by the coarse axes (dt beta_out / h_x^2 =
+    2.5e5): the forward multipliers sit within 1/sqrt(kappa) of 1, so FP32
+    rounding accumulates along a line (as in any FP32 recurrence) to about
+    n eps_32.  Tolerance 4 n eps_32 of the plain form, and the accuracy
+    contract against the exact solution."""
+    n = (400, 33, 35)
+    spec = M.Spec(n=n, surface="ellipsoid", surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
+                  beta_in=1.0, beta_out=100.0, method="adi", mib=2, dt=2.0 / (min(n) - 1))
+    u_p, (l_p, _, _) = run(spec, "plain", 4)
+    u_m, (l_m, _, _) = run(spec, "mixed", 4)
+    assert rel_maxdiff(u_m, u_p) <= 4 * n[0] * 2.0 ** -24
+    assert l_m <= LINF_RATIO * l_p and l_p <= LINF_RATIO * l_m
+
+
 def test_mixed_rejects_other_methods():
     spec = M.Spec(n=(33, 33, 33), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=10.0,
                   method="lod-cn", mib=2, dt=1.0 / 16)
