@@ -88,8 +88,9 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served-form run")
     ap.add_argument("--batch-problems", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=50)
-    ap.add_argument("--served-requests", type=int, default=1000,
-                    help="requests per arrival rate (the full served workload is 10000)")
+    ap.add_argument("--served-requests", type=int, default=3000,
+                    help="requests per arrival rate (3000: the 1000 req/s stream reaches its steady state; "
+                         "the full served workload is 10000)")
     ap.add_argument("--served-rates", default="200,1000", help="Poisson arrival rates, requests/s")
     ap.add_argument("--workload", default="step", choices=["step", "precision", "batched", "served"],
                     help="step: the headline line (default); precision / batched / served: the full sweep of "
