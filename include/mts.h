@@ -237,8 +237,20 @@ mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
  * against the exact solution stays that of the plain form.  Switching the
  * form on builds its per-node FP32 coefficients on the device once (3 x 4
  * bytes per node and direction, for lines of up to 544 rows).  No
- * counterpart in the reference, which computes in FP64 only. */
-typedef enum { MTS_PRECISION_PLAIN = 0, MTS_PRECISION_MIXED = 1 } mts_precision;
+ * counterpart in the reference, which computes in FP64 only.
+ *
+ * MTS_PRECISION_FAST (Douglas-ADI only, at most 544 nodes per axis) is the
+ * same step in FP64 throughout, reorganised for the GPU: it is solved for the
+ * increment as above, with the residual formed inside the x sweep, and every
+ * line is solved by one warp whose lanes split the Thomas recurrences into
+ * segments joined by shuffle scans.  The operations are those of the plain
+ * form in another order, so results differ from it by rounding only (within
+ * 1e-10 relative max-norm over the runs the tests cover).  Switching it on
+ * builds its row tables and, for lines that cross the interface, 32 factor
+ * checkpoints per line (16 bytes each) on the device once.  Profiling slots
+ * of this form: {0 residual + x solve, 1 y solve, 2 z solve + update}.
+ * No counterpart in the reference, which computes in FP64 only. */
+typedef enum { MTS_PRECISION_PLAIN = 0, MTS_PRECISION_MIXED = 1, MTS_PRECISION_FAST = 2 } mts_precision;
 mts_status mts_set_precision(mts_handle h, int32_t precision);
 mts_status mts_get_precision(mts_handle h, int32_t* precision);
 

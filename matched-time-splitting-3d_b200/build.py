@@ -5,7 +5,8 @@
 Host code (setup, C ABI) and device code are compiled without floating-point
 contraction (-fmad=false for the device, -ffp-contract=off for the host): the
 plain FP64 path must round every product and sum on its own, as the reference
-CPU build does.
+CPU build does.  The fast FP64 form (fast.cu), whose results are only required
+to match the reference to rounding, is compiled with fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -19,10 +20,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmts_b200.so")
-SOURCES = ["setup.cpp", "kernels.cu", "mixed.cu", "capi.cu"]
+SOURCES = ["setup.cpp", "kernels.cu", "mixed.cu", "fast.cu", "capi.cu"]
 HEADERS = ["setup.h", "device.h", "device_common.cuh"]
 OBJ_DIR = os.path.join(HERE, "build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# device code of these sources may contract a*b+c into one fused multiply-add
+FMA_SOURCES = {"fast.cu"}
 
 
 def nvcc() -> str:
@@ -58,7 +61,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     def compile_one(src):
         obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
-        cmd = [nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj]
+        fl = [("-fmad=true" if f == "-fmad=false" and src in FMA_SOURCES else f) for f in flags]
+        cmd = [nvcc(), *fl, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         cp = subprocess.run(cmd, capture_output=True, text=True)

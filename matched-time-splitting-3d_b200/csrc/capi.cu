@@ -80,7 +80,10 @@ struct mts_problem {
   double prof_ms[mts::kProfileSlots] = {};
   int64_t prof_n[mts::kProfileSlots] = {};
 
-  int slots() const { return prm.method == MTS_TS ? 6 : prm.method == MTS_ADI ? 5 : 4; }
+  int slots() const {
+    if (dev.precision == 2) return 3;
+    return prm.method == MTS_TS ? 6 : prm.method == MTS_ADI ? 5 : 4;
+  }
 
   ~mts_problem() {
     if (stream) cudaStreamSynchronize(stream);
@@ -440,6 +443,7 @@ mts_status finish_create(mts_problem* h) {
     mts::configure_kernels();
     mts::configure_mixed_kernels();
     mts::configure_batch_kernels();
+    mts::configure_fast_kernels();
     configured = true;
   }
   int sms = 0;
@@ -526,7 +530,9 @@ mts_status finish_create(mts_problem* h) {
     D.precision = 0;
   }
   uint8_t* dtag = nullptr;
-  CUDA_TRY(h->put(&dtag, tag8.data(), tag8.size()));
+  // (slack past the end: the fast form's bulk copies of tag rows may run
+  // past the last row of the last plane)
+  CUDA_TRY(h->put_padded(&dtag, tag8.data(), tag8.size(), fpad));
   D.tag = dtag;
   {
     // nodes that are a MIB row of some block: the pointwise passes leave them
@@ -624,7 +630,9 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
     ev = h->ev_busy.back().data();
   }
   CUDA_TRY(ensure_side_stream(h));
-  if (h->dev.precision == 1)
+  if (h->dev.precision == 2)
+    h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, ev);
+  else if (h->dev.precision == 1)
     h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev, &h->side);
   else
     h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, ev, &h->side);
@@ -649,6 +657,7 @@ mts_status sync_status(mts_problem* h) {
   CUDA_TRY(cudaMemcpyAsync(&flag, h->dev.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   if (flag & 1) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line solve");
+  if (flag & 2) return fail(MTS_ERR_CUDA, "a device-side wait for a bulk copy timed out");
   return MTS_OK;
 }
 
@@ -932,7 +941,9 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     BATCH_TRY(ensure_side_stream(h));
     for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
-      if (h->dev.precision == 1)
+      if (h->dev.precision == 2)
+        h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, nullptr);
+      else if (h->dev.precision == 1)
         h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
       else
         h->launches += mts::launch_step(h->dev, T, h->u0, h->u1, h->stream, nullptr, &h->side);
@@ -1141,8 +1152,33 @@ mts_status mts_set_sweep_shape(mts_handle h, int32_t sweep, int32_t shape) {
 
 mts_status mts_set_precision(mts_handle h, int32_t precision) {
   if (!h) return fail(MTS_ERR_ARG, "null handle");
-  if (precision != MTS_PRECISION_PLAIN && precision != MTS_PRECISION_MIXED)
-    return fail(MTS_ERR_ARG, "precision must be MTS_PRECISION_PLAIN or MTS_PRECISION_MIXED");
+  if (precision != MTS_PRECISION_PLAIN && precision != MTS_PRECISION_MIXED && precision != MTS_PRECISION_FAST)
+    return fail(MTS_ERR_ARG, "precision must be MTS_PRECISION_PLAIN, MTS_PRECISION_MIXED or MTS_PRECISION_FAST");
+  if (precision == MTS_PRECISION_FAST) {
+    if (h->prm.method != MTS_ADI) return fail(MTS_ERR_ARG, "the fast FP64 form is built for Douglas-ADI only");
+    if (!mts::fast_fits(h->g.nx, h->g.ny, h->g.nz))
+      return fail(MTS_ERR_ARG, "grid lines too long for the fast FP64 form (at most 544 nodes per axis)");
+    if (!h->dev.ftab[0]) {
+      // row tables and lane checkpoints, once per handle
+      const int nd[3] = {h->g.nx, h->g.ny, h->g.nz};
+      for (int d = 0; d < 3; d++) {
+        const size_t R = 32 * (size_t)mts::fast_rows_per_lane(nd[d]);
+        double* tab = nullptr;
+        CUDA_TRY(h->put(&tab, (const double*)nullptr, 6 * R));
+        h->dev.ftab[d] = tab;
+        mts::FastChk* chk = nullptr;
+        if (h->nblk[d] > 0) {
+          const size_t nck = 32 * (size_t)line_count(h->g, d);
+          CUDA_TRY(h->put(&chk, (const mts::FastChk*)nullptr, nck));
+          CUDA_TRY(cudaMemsetAsync(chk, 0, nck * sizeof(mts::FastChk), h->stream));
+        }
+        h->dev.fchk[d] = chk;
+      }
+      mts::build_fast_tables(h->dev, h->stream);
+      CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+  }
   if (precision == MTS_PRECISION_MIXED) {
     if (h->prm.method != MTS_ADI) return fail(MTS_ERR_ARG, "the mixed-precision form is built for Douglas-ADI only");
     const int nmax = std::max(h->g.nx, std::max(h->g.ny, h->g.nz));
@@ -1180,6 +1216,12 @@ mts_status mts_get_precision(mts_handle h, int32_t* precision) {
 
 mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]) {
   if (!h || steps < 1) return fail(MTS_ERR_ARG, "bad argument");
+  if (h->dev.precision != MTS_PRECISION_PLAIN) {
+    // the shapes are those of the bit-exact sweeps; the other forms have none
+    if (shapes)
+      for (int k = 0; k < 3; k++) shapes[k] = h->dev.shape[k];
+    return MTS_OK;
+  }
   const size_t bytes = sizeof(double) * (size_t)h->g.nodes();
   double* backup = nullptr;
   CUDA_TRY(cudaMalloc((void**)&backup, bytes));

@@ -252,11 +252,13 @@ class Solver:
     def set_sweep_shape(self, sweep: int, shape: int) -> None:
         check(self._L.mts_set_sweep_shape(self._h, int(sweep), int(shape)), "mts_set_sweep_shape")
 
-    PRECISIONS = {"plain": 0, "mixed": 1}
+    PRECISIONS = {"plain": 0, "mixed": 1, "fast": 2}
 
     def set_precision(self, precision: str) -> None:
-        """"plain" (FP64, bit-identical to the reference) or "mixed" (FP32
+        """"plain" (FP64, bit-identical to the reference), "mixed" (FP32
         line solves on the step's increment, FP64 residual and state;
+        Douglas-ADI only) or "fast" (FP64 throughout, warp-segmented line
+        solves of the increment, equal to the plain form up to rounding;
         Douglas-ADI only)."""
         check(self._L.mts_set_precision(self._h, self.PRECISIONS[precision]), "mts_set_precision")
 
