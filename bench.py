@@ -1,12 +1,14 @@
 #!/usr/bin/env python
-"""Benchmark of the plain FP64 GPU time step (cell-steps/s at 257^3).
+"""Benchmark of the FP64 GPU time step (cell-steps/s at 257^3).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload (default): the 257^3-node grid on [-1,1]^3 (h = 1/128, the "256^3"
 of the headline metric), Douglas-ADI + MIB-L2, torus R=0.5 r=0.2, beta 1:1000,
-exact solution e^{-t}(...) (eq 8), dt = h, plain FP64.  A "step" is one time
-step of that problem.  Each field is 136 MB and a step streams ~1 GB, larger
+exact solution e^{-t}(...) (eq 8), dt = h, FP64.  A "step" is one time step
+of that problem, computed by the fast FP64 form (MTS_PRECISION_FAST: FP64
+throughout, equal to the reference up to rounding); the bit-exact plain form
+is timed beside it.  Each field is 136 MB and a step streams ~1 GB, larger
 than the 126 MB L2, so no explicit L2 flush is needed between steps.
 
 Multi-GPU: one independent replica per rank (the path does not shard; no
@@ -33,6 +35,12 @@ sys.path.insert(0, os.path.join(ROOT, "matched-time-splitting-3d_b200"))
 WORKLOAD = dict(n=(257, 257, 257), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=1000.0, eq=8,
                 method="adi", mib=2, dt=2.0 / 256)
 METRIC = "cell-steps/s @256^3 plain FP64"
+# Algorithmic bytes per node and step of the fast FP64 form: the residual
+# with the x solve (read u^n 8 + tag 1, write d* 8), the y solve in place
+# (read 8, write 8), the z solve with the update (read d** 8, read u^n 8,
+# write u^{n+1} 8).
+FAST_BYTES = {0: 17, 1: 16, 2: 24}
+FAST_NAMES = ["fast_x_residual_and_solve", "fast_y_solve", "fast_z_solve_and_update"]
 REF_MAX_STEPS = 3  # timed steps per reference process (CPU arm)
 # Algorithmic bytes per node and step of the mixed ADI form: residual (read
 # u^n 8 + tag 1, write rho 4), x and y FP32 solves (read 4, write 4 each),
@@ -82,6 +90,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: auto)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default sweep shapes")
+    ap.add_argument("--precision", default="auto", choices=["auto", "fast", "plain"],
+                    help="arithmetic of the headline step: fast (FP64, reordered; Douglas-ADI) or plain "
+                         "(bit-identical to the reference); auto = fast where the form applies")
+    ap.add_argument("--no-exact", action="store_true", help="skip the bit-exact plain form run beside the fast one")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run (ADI only)")
     ap.add_argument("--shapes", default="", help="sweep shapes of the three sweeps, e.g. 4,4,4 (no autotune)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form run")
@@ -261,10 +273,10 @@ def workload(a):
     return w
 
 
-def config_of(w, world):
+def config_of(w, world, form="plain"):
     return {
         "workload": f"{w['n'][0]}^3 {w['method']} MIB-L{w['mib']} {w['surface']}{tuple(w['surface_params'])} "
-                    f"beta {w['beta_in']}:{w['beta_out']} eq{w['eq']} dt=h plain FP64",
+                    f"beta {w['beta_in']}:{w['beta_out']} eq{w['eq']} dt=h plain FP64 ({form} form)",
         "grid": list(w["n"]),
         "method": w["method"],
         "mib": w["mib"],
@@ -477,16 +489,24 @@ def main():
     import mts_b200 as M
 
     spec = M.Spec(**w)
+    prec = a.precision
+    if prec == "auto":
+        prec = "fast" if w["method"] == "adi" else "plain"
     solver = M.Solver(spec)
+    solver.set_precision(prec)
     solver.initialize()
-    if a.shapes:
-        shapes = tuple(int(v) for v in a.shapes.split(","))
-        for k, v in enumerate(shapes):
-            solver.set_sweep_shape(k, v)
-    elif a.no_autotune:
-        shapes = ("default",)
-    else:
-        shapes = solver.autotune(2)
+
+    def plain_shapes(sv):
+        if a.shapes:
+            sh = tuple(int(v) for v in a.shapes.split(","))
+            for k, v in enumerate(sh):
+                sv.set_sweep_shape(k, v)
+            return sh
+        if a.no_autotune:
+            return ("default",)
+        return sv.autotune(2)
+
+    shapes = plain_shapes(solver) if prec == "plain" else ("none: the fast form has no sweep shapes",)
     solver.advance(a.warmup)
     solver.synchronize()
 
@@ -516,8 +536,9 @@ def main():
     solver.set_profiling(False)
     launches = solver.launch_count() - launches0
     lmax, l2, _ = solver.norms()
-    t_plain = solver.time
-    u_plain = solver.solution() if (w["method"] == "adi" and not a.no_mixed) else None
+    t_head = solver.time
+    u_head = solver.solution() if w["method"] == "adi" and (not a.no_mixed or (prec == "fast" and not a.no_exact)) \
+        else None
 
     # end to end through the C ABI with host buffers: the field goes up and
     # comes back every step (the reference's Solve_2nd contract on a host
@@ -541,38 +562,65 @@ def main():
     value = job_value(world, nodes, a.steps, ms_max)
     e2e_value = job_value(world, nodes, e2e_steps, e2e_max)
 
+    def timed_run(precision):
+        """Another handle on the same workload: warm-up, then the same K
+        steps from the same start, so that its solution is compared with the
+        headline's at the same time.  Returns (ms, kernel ms, launches,
+        norms, solution, shapes)."""
+        sv = M.Solver(spec)
+        sv.set_precision(precision)
+        sv.initialize()
+        sh = plain_shapes(sv) if precision == "plain" else None
+        sv.advance(a.warmup)
+        sv.synchronize()
+        st_ = torch.cuda.ExternalStream(sv.stream())
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        sv.set_profiling(True)
+        sv.profile_read()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        m0.record(st_)
+        sv.advance(a.steps)
+        m1.record(st_)
+        sv.synchronize()
+        ms_ = m0.elapsed_time(m1)
+        km, kc = sv.profile_read()
+        sv.set_profiling(False)
+        nr = sv.norms()
+        u_ = sv.solution()
+        assert sv.time == t_head
+        sv.close()
+        (ms_,) = max_over_ranks([ms_], dist)
+        return ms_, km, kc, nr, u_, sh
+
+    def rel(u_, ref):
+        return float(abs(u_ - ref).max() / max(1e-300, abs(ref).max()))
+
+    # The bit-exact plain form on the same workload (the drop-in arithmetic,
+    # bit-identical to the reference), beside the fast form.
+    exact = None
+    if prec == "fast" and not a.no_exact and u_head is not None:
+        ms_e, km_e, kc_e, (le, l2e, _), ue, sh_e = timed_run("plain")
+        v_e = job_value(world, nodes, a.steps, ms_e)
+        exact = {
+            "value": v_e, "unit": "cell-steps/s", "ms_per_step": ms_e / a.steps, "sweep_shapes": list(sh_e),
+            "fast_speedup": value / v_e, "lmax": le, "l2": l2e,
+            "fast_rel_maxdiff": rel(u_head, ue), "fast_lmax_rel_diff": abs(lmax - le) / le,
+            "kernels": {nm: {"ms_per_launch": km_e[k] / kc_e[k], "launches": int(kc_e[k])}
+                        for k, nm in enumerate(SLOT_NAMES["adi"]) if kc_e[k] > 0},
+            "form": "MTS_PRECISION_PLAIN: the reference's operations in the reference's order (bit-identical); "
+                    "fast_rel_maxdiff = max|u_fast - u_exact| / max|u_exact| after the same warm-up + timed steps",
+        }
+        del ue
+
     # The mixed-precision form (FP32 line solves on the increment, FP64
     # residual and state) on the same workload, same steps from the same
     # start, so its error is compared at the same time.
     mixed = None
-    if u_plain is not None:
-        sm = M.Solver(spec)
-        sm.set_precision("mixed")
-        sm.initialize()
-        sm.advance(a.warmup)
-        sm.synchronize()
-        stream_m = torch.cuda.ExternalStream(sm.stream())
-        m0 = torch.cuda.Event(enable_timing=True)
-        m1 = torch.cuda.Event(enable_timing=True)
-        sm.set_profiling(True)
-        sm.profile_read()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        m0.record(stream_m)
-        sm.advance(a.steps)
-        m1.record(stream_m)
-        sm.synchronize()
-        ms_m = m0.elapsed_time(m1)
-        kms_m, kn_m = sm.profile_read()
-        sm.set_profiling(False)
-        lm, l2m, _ = sm.norms()
-        um = sm.solution()
-        rel = float(abs(um - u_plain).max() / max(1e-300, abs(u_plain).max()))
-        assert sm.time == t_plain
-        sm.close()
-        del um
-        (ms_m,) = max_over_ranks([ms_m], dist)
+    if u_head is not None and not a.no_mixed:
+        ms_m, kms_m, kn_m, (lm, l2m, _), um, _ = timed_run("mixed")
         v_m = job_value(world, nodes, a.steps, ms_m)
         # the jumps and the residual's MIB rows run on a side stream beside
         # the pointwise residual: the first slot is that stream's jumps
@@ -581,37 +629,41 @@ def main():
         names_m = ["jumps_side_stream", "residual_fp64", "x_solve_fp32", "y_solve_fp32", "z_solve_fp32_and_accumulate"]
         mixed = {
             "value": v_m, "unit": "cell-steps/s", "ms_per_step": ms_m / a.steps,
-            "speedup_vs_plain": v_m / (world * nodes * a.steps / (ms / 1e3)),
+            "speedup_vs_plain": v_m / value,
+            "speedup_vs_exact_plain": (v_m / exact["value"]) if exact else None,
             "lmax": lm, "l2": l2m, "lmax_plain": lmax, "l2_plain": l2, "lmax_ratio": lm / lmax,
-            "rel_maxdiff_vs_plain": rel, "t": t_plain,
+            "rel_maxdiff_vs_plain": rel(um, u_head), "t": t_head,
             "bytes_per_node_step": MIXED_BYTES,
             "step_roofline_frac": MIXED_BYTES * nodes * a.steps / (ms_m / 1e3) / 1e9 / peak_hbm(),
             "kernels": {n: {"ms_per_launch": kms_m[k] / kn_m[k], "launches": int(kn_m[k])}
                         for k, n in enumerate(names_m) if kn_m[k] > 0},
             "form": "residual dt(A_x+A_y+A_z)u^n + dt src in FP64, three segmented FP32 line solves of the "
                     "increment (warp per line, lane segments joined by shuffle scans), FP64 state += increment "
-                    "in the z solve",
+                    "in the z solve; speedup_vs_plain is against the headline (fast FP64) form",
         }
+        del um
 
     method = w["method"]
-    names = SLOT_NAMES[method]
+    if prec == "fast":
+        names, alg = FAST_NAMES, FAST_BYTES
+    else:
+        names, alg = SLOT_NAMES[method], ALG_BYTES[method]
     kernels = {}
     for k, name in enumerate(names):
         if kn[k] > 0:
             kernels[name] = {"ms_per_launch": kms[k] / kn[k], "launches": int(kn[k]),
                              "share": kms[k] / max(1e-12, kms[: len(names)].sum())}
-    dom = max((k for k in ALG_BYTES[method]), key=lambda k: kms[k])
+    dom = max((k for k in alg), key=lambda k: kms[k])
     peak, peak_src = peak_hbm(), ("measured" if os.path.exists(PEAKS_PATH) else "fallback")
     per_launch_ms = kms[dom] / kn[dom]
-    achieved = ALG_BYTES[method][dom] * nodes / (per_launch_ms / 1e3) / 1e9
-    step_bytes = sum(ALG_BYTES[method].values())
+    achieved = alg[dom] * nodes / (per_launch_ms / 1e3) / 1e9
+    step_bytes = sum(alg.values())
     roofline = {
         "bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})",
         "traffic": None,
-        "algorithmic_bytes_per_node": ALG_BYTES[method][dom],
-        # the contract's step model counts the first RHS fused into the x
-        # sweep: 67 B per node-step for ADI (51 LOD, 102 TS)
+        "algorithmic_bytes_per_node": alg[dom],
+        # the contract's step model: 67 B per node-step for ADI (51 LOD, 102 TS)
         "step_contract": {"bytes_per_node_step": CONTRACT_BYTES[method],
                           "frac": CONTRACT_BYTES[method] * nodes * a.steps / (ms / 1e3) / 1e9 / peak},
         "step": {"bytes_per_node_step": step_bytes,
@@ -630,13 +682,16 @@ def main():
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic exact solution, seeded geometry)",
-        "config": config_of(w, world), "gpu_launches": int(launches), "kernels": kernels, "roofline": roofline,
-        "sweep_shapes": list(shapes),
+        "precision_form": prec,
+        "config": config_of(w, world, prec), "gpu_launches": int(launches), "kernels": kernels,
+        "roofline": roofline, "sweep_shapes": list(shapes),
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * nodes,
                 "d2h_bytes_per_step": 8 * nodes, "steps": e2e_steps,
                 "api": "mts_advance_host (field uploaded and downloaded every step, pinned host memory)"},
-        "clocks": clk, "accuracy": {"lmax": lmax, "l2": l2, "t": t_plain},
+        "clocks": clk, "accuracy": {"lmax": lmax, "l2": l2, "t": t_head},
     }
+    if exact is not None:
+        line["exact_plain"] = exact
     if mixed is not None:
         line["mixed"] = mixed
     if rank == 0 and world == 1 and not a.no_batched:
