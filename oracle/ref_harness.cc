@@ -27,7 +27,9 @@
 
 #include "constant.h"
 #include "diffusion/beta.h"
+#include "diffusion/beta_1.h"
 #include "equation/eq_0.h"
+#include "equation/eq_3.h"
 #include "equation/equation.h"
 #include "mesh/mesh.h"
 #include "spatial/intersection.h"
@@ -167,13 +169,14 @@ struct Args {
   string dump_u, dump_tags, dump_mib, dump_u0;
   string report;     // --report F: the stepper's own Error() text at the end
   bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
+  int beta_plugin = -1;  // --beta-plugin 1: the reference's Beta_1 instead of the piecewise-constant beta
 };
 
 [[noreturn]] void usage() {
   fprintf(stderr,
           "mts_ref --n NX NY NZ --domain xl xr yl yr zl zr\n"
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
-          "        --beta bi bo --eq 0|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
+          "        --beta bi bo [--beta-plugin 1] --eq 0|3|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
           "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F]\n"
 #ifdef MTS_DROPIN
@@ -205,6 +208,9 @@ Args parse(int argc, char** argv) {
       need(2);
       a.bi = atof(argv[++i]);
       a.bo = atof(argv[++i]);
+    } else if (k == "--beta-plugin") {
+      need(1);
+      a.beta_plugin = atoi(argv[++i]);
     } else if (k == "--eq") {
       need(1);
       a.eq = atoi(argv[++i]);
@@ -255,6 +261,7 @@ Args parse(int argc, char** argv) {
 unique_ptr<Equation> make_eq(const Args& a, double t, Beta& beta) {
   if (a.eq == 8) return unique_ptr<Equation>(new Eq8(t, a.bi, a.bo));
   if (a.eq == 0) return unique_ptr<Equation>(new Eq_0(t, beta));
+  if (a.eq == 3) return unique_ptr<Equation>(new Eq_3(t, beta));
   fprintf(stderr, "unsupported --eq %d\n", a.eq);
   exit(2);
 }
@@ -340,7 +347,14 @@ int main(int argc, char** argv) {
   } else {
     usage();
   }
-  PiecewiseBeta beta(a.bi, a.bo);
+  unique_ptr<Beta> beta_own;
+  if (a.beta_plugin == 1)
+    beta_own.reset(new Beta_1());
+  else if (a.beta_plugin < 0)
+    beta_own.reset(new PiecewiseBeta(a.bi, a.bo));
+  else
+    usage();
+  Beta& beta = *beta_own;
 
   VecDoub domain(a.dom, a.dom + 6);
   VecInt size{a.n[0], a.n[1], a.n[2]};
@@ -445,13 +459,20 @@ int main(int argc, char** argv) {
 #ifdef MTS_DROPIN
   if (a.gpu) {
     int method = a.method == "adi" ? MTS_ADI : a.method == "lod-ie" ? MTS_LOD_IE : a.method == "lod-cn" ? MTS_LOD_CN : MTS_TS;
-    mts::GpuStepper st(inter, mesh, beta, time, 2, method, a.eq);
-    if (a.method == "adi")
-      run(st, adi_step);
-    else if (lod)
-      run(st, lod_step);
-    else
-      run(st, ts_step);
+    try {
+      // (the stepper is told eq 8 for any Equation the loop builds other than
+      // Eq_0: it must refuse the ones it does not evaluate)
+      mts::GpuStepper st(inter, mesh, beta, time, 2, method, a.eq == 0 ? 0 : 8);
+      if (a.method == "adi")
+        run(st, adi_step);
+      else if (lod)
+        run(st, lod_step);
+      else
+        run(st, ts_step);
+    } catch (const std::exception& e) {
+      fprintf(stderr, "mts_dropin: %s\n", e.what());
+      return 3;
+    }
   } else
 #endif
   if (a.method == "adi") {

@@ -3,7 +3,7 @@ own time-stepping code (oracle/_ref/mts_ref, built from the reference sources
 by oracle/Makefile).  Needs the reference tree; the GPU box only reads the
 committed .npz files.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference checkout> && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
