@@ -266,7 +266,7 @@ class Solver:
     def precision(self) -> str:
         v = ctypes.c_int32()
         check(self._L.mts_get_precision(self._h, ctypes.byref(v)), "mts_get_precision")
-        return {0: "plain", 1: "mixed"}[v.value]
+        return {v_: k for k, v_ in self.PRECISIONS.items()}[v.value]
 
     def autotune(self, steps: int = 2):
         """Times every compiled sweep shape on this problem and keeps the
