@@ -246,9 +246,10 @@ mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
  * segments joined by shuffle scans.  The operations are those of the plain
  * form in another order, so results differ from it by rounding only (within
  * 1e-10 relative max-norm over the runs the tests cover).  Switching it on
- * builds its row tables and, for lines that cross the interface, 32 factor
- * checkpoints per line (16 bytes each) on the device once.  Profiling slots
- * of this form: {0 residual + x solve, 1 y solve, 2 z solve + update}.
+ * builds its row tables and, for each line that crosses the interface, its
+ * per-row solve coefficients (3 x 8 bytes per row) on the device once.
+ * Profiling slots of this form: {0 MIB rows + residual + x solve, 1 y solve,
+ * 2 z solve + update}.
  * No counterpart in the reference, which computes in FP64 only. */
 typedef enum { MTS_PRECISION_PLAIN = 0, MTS_PRECISION_MIXED = 1, MTS_PRECISION_FAST = 2 } mts_precision;
 mts_status mts_set_precision(mts_handle h, int32_t precision);

@@ -657,7 +657,6 @@ mts_status sync_status(mts_problem* h) {
   CUDA_TRY(cudaMemcpyAsync(&flag, h->dev.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   if (flag & 1) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line solve");
-  if (flag & 2) return fail(MTS_ERR_CUDA, "a device-side wait for a bulk copy timed out");
   return MTS_OK;
 }
 
@@ -1159,20 +1158,34 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
     if (!mts::fast_fits(h->g.nx, h->g.ny, h->g.nz))
       return fail(MTS_ERR_ARG, "grid lines too long for the fast FP64 form (at most 544 nodes per axis)");
     if (!h->dev.ftab[0]) {
-      // row tables and lane checkpoints, once per handle
+      // row tables, and the coefficients of the lines that cross the
+      // interface (numbered in line order), once per handle
       const int nd[3] = {h->g.nx, h->g.ny, h->g.nz};
       for (int d = 0; d < 3; d++) {
         const size_t R = 32 * (size_t)mts::fast_rows_per_lane(nd[d]);
         double* tab = nullptr;
         CUDA_TRY(h->put(&tab, (const double*)nullptr, 6 * R));
         h->dev.ftab[d] = tab;
-        mts::FastChk* chk = nullptr;
-        if (h->nblk[d] > 0) {
-          const size_t nck = 32 * (size_t)line_count(h->g, d);
-          CUDA_TRY(h->put(&chk, (const mts::FastChk*)nullptr, nck));
-          CUDA_TRY(cudaMemsetAsync(chk, 0, nck * sizeof(mts::FastChk), h->stream));
-        }
-        h->dev.fchk[d] = chk;
+        h->dev.fcoef[d] = nullptr;
+        h->dev.fcidx[d] = nullptr;
+        if (h->nblk[d] == 0) continue;
+        const size_t nl = (size_t)line_count(h->g, d);
+        std::vector<int32_t> bs(nl + 1), cidx(nl, -1);
+        CUDA_TRY(cudaMemcpyAsync(bs.data(), h->dev.bstart[d], bs.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        int32_t nc = 0;
+        for (size_t l = 0; l < nl; l++)
+          if (bs[l + 1] > bs[l]) cidx[l] = nc++;
+        int32_t* dci = nullptr;
+        CUDA_TRY(h->put(&dci, cidx.data(), nl));
+        double* cf = nullptr;
+        CUDA_TRY(h->put(&cf, (const double*)nullptr, 3 * R * (size_t)nc));
+        CUDA_TRY(cudaMemsetAsync(cf, 0, 3 * R * (size_t)nc * sizeof(double), h->stream));
+        h->dev.fcidx[d] = dci;
+        h->dev.fcoef[d] = cf;
+        // the host vector must outlive the asynchronous upload
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
       }
       mts::build_fast_tables(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());

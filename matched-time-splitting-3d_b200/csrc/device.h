@@ -60,15 +60,6 @@ struct CrossConst {
   double pinv;
 };
 
-// Fast FP64 form: where lane l of a warp starts its segment (row l*MX) of a
-// line that crosses the interface: bet of that row, the side of the regular
-// rows there, and the first block that ends at or after it.
-struct FastChk {
-  double bet;
-  int32_t side;
-  int32_t blk;
-};
-
 struct Dev {
   int nx, ny, nz;
   int eq, method;
@@ -132,10 +123,12 @@ struct Dev {
   int precision;              // 0 plain FP64, 1 mixed, 2 fast FP64
   // Fast FP64 form (segmented line solves, fast.cu), built when the form is
   // switched on: per direction, the row tables [side][1/bet, -a/bet,
-  // -gam_{j+1}][32 MX] of the lines without crossings, and the lane
-  // checkpoints [line][32] of the lines that cross the interface.
+  // -gam_{j+1}][32 MX] of the lines without crossings, and the same three
+  // values per row for each line that crosses the interface,
+  // fcoef[c][3][32 MX], c = fcidx[line] (-1 for the other lines).
   const double* ftab[3];
-  const FastChk* fchk[3];
+  const double* fcoef[3];
+  const int32_t* fcidx[3];
   // Replayable steps (batches captured in a CUDA graph): when tsched is set,
   // kernels take the step's exp(-t) factors from tsched[3*(*tstep) + {0: t_prev,
   // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
@@ -192,7 +185,7 @@ int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cud
 void configure_fast_kernels();
 int fast_rows_per_lane(int n);               // MX of a direction with n rows (0: lines too long)
 bool fast_fits(int nx, int ny, int nz);      // the form takes this grid
-int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab / fchk (allocated by the caller)
+int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab / fcoef (allocated by the caller)
 // Batched plain steps (kernels.cu): problems of one method advance together,
 // one launch per kernel of the step for all of them.  A launch's CTAs are
 // listed as items (problem, the CTA's index in that problem's own grid, the

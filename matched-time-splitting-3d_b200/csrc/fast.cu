@@ -8,25 +8,26 @@
 // with d = Outer_u(t^{n+1}) - u^n on the faces (A_d = dt beta D_dd with the
 // MIB rows, src = f plus the jump terms of Src_2nd, douglas_adi.cc:1123-1428).
 // Everything here is FP64; the result differs from the reference's sequence
-// of operations only by rounding.  A step is three launches:
+// of operations only by rounding.  A step is four launches:
 //
-//   kf_x   the residual rho fused with the x line solves.  A CTA owns TY
-//          neighbouring x lines (rows iy0..iy0+TY-1) and walks a range of z
-//          planes.  Plane by plane it brings the TY+2 rows of u^n around its
-//          lines (one contiguous run of memory) and their tags into shared
-//          memory with one bulk copy each (cp.async.bulk, completion on an
-//          mbarrier), four planes in a ring, so that the z-1, z and z+1 rows
-//          of the stencil all come from shared memory and the copy of plane
-//          z+2 is in flight while plane z is computed.  Warp w forms rho of
-//          line iy0+w (the MIB rows with their fictitious-point sums and jump
-//          terms included), applies the Convert2Tri row operations of the
-//          line's blocks (douglas_adi.cc:1554-1675), solves the line and
-//          writes d* to global memory.
+//   kf_mib the right-hand side of every MIB row (the explicit MIB sums of all
+//          three directions and the jump terms, one thread per node; the
+//          Convert2Tri row operations of the x blocks, one thread per
+//          block), written into the d field at those nodes.  Their
+//          dependent table walks run here, spread over many threads, and not
+//          inside the line solves.
+//   kf_x   rho fused with the x line solves: warp w of a CTA takes one x
+//          line at a time (the CTA's warps take a 4 x 2 block of lines, so
+//          that a line's y and z neighbours are mostly its siblings' lines
+//          and come from L1), forms rho of its rows from coalesced loads of
+//          u^n (taking the MIB rows from kf_mib), solves the line in shared
+//          memory and writes d*.
 //   kf_yz  the y solve in place on d*, and the z solve with the accumulation
 //          u^{n+1} = u^n + d.  A CTA copies NL neighbouring lines (the same
 //          row of NL lines is NL consecutive doubles) into shared memory,
 //          double-buffered so that the next tile's copy overlaps this tile's
-//          solves, and warp w solves line w.
+//          solves, and warp w solves line w (the Convert2Tri row operations
+//          of its blocks first, douglas_adi.cc:1554-1675).
 //
 // Line solve: with the Thomas factors fixed (bet_j, gam_j of TDMA,
 // douglas_adi.cc:1784-1807), both recurrences are first-order and linear:
@@ -36,10 +37,9 @@
 // rows [l MX, l MX + MX); each lane runs its rows from a zero carry, the
 // lanes' affine end maps are composed by a shuffle scan, and a second pass
 // runs the rows again from the true carry.  Lines without crossings read
-// (ib, p, q) from per-side row tables; a line that crosses the interface
-// recomputes its factors from the block rows (bet_j = b_j + a_j q_{j-1},
-// q_j = -c_j / bet_j), each lane starting from the stored bet of its first
-// row, so no per-node factor field is read.
+// (ib, p, q) from per-side row tables in shared memory; the lines that cross
+// the interface read their own, stored line after line ([line][ib, p, q][row]),
+// so that each lane loads its rows' 27 values in one round.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,50 +51,7 @@ namespace mts {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int X_NFACE = 8;   // CTAs of kf_x that fill the face lines
 constexpr int YZ_NL = 8;     // lines per tile of kf_yz (one warp each)
-constexpr long long kWaitCycles = 1LL << 32;  // ~2 s of SM clock: a bulk copy that has not landed by then never will
-
-// ---------------------------------------------------------------------------
-// Bulk copies into shared memory with mbarrier completion
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-// src and dst 16-byte aligned, bytes a multiple of 16
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Waits for the phase of the given parity to complete, giving up after
-// kWaitCycles clocks of this SM.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  if (mbar_test(bar, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_test(bar, parity))
-    if (clock64() - t0 > kWaitCycles) return false;
-  return true;
-}
-// Orders this thread's generic-proxy shared-memory accesses before later
-// bulk copies into the same memory.
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Jump data on the fly (Refresh_Jump, intersection.cc:2294-2490): [u] and
@@ -232,11 +189,10 @@ __device__ __forceinline__ double carry_down(double A, double B, int lane) {
   return lane == 31 ? 0.0 : X;
 }
 
-// A line without crossings: (ib, p, q) from the row table of its side,
-// tab[0..R) = ib, tab[R..2R) = p, tab[2R..3R) = q (zero past the line end).
-template <int MX>
-__device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n, int lane) {
-  constexpr int R = 32 * MX;
+// The segmented solve proper; IB(k), PP(k), QQ(k) give ib, p, q of the
+// lane's row jb + k (zero past the line end).
+template <int MX, class FI, class FP, class FQ>
+__device__ __forceinline__ void solve_seg(double* buf, int n, int lane, FI IB, FP PP, FQ QQ) {
   const int jb = lane * MX;
   double y[MX];
   double B = 0.0, A = 1.0;
@@ -244,8 +200,8 @@ __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n,
   for (int k = 0; k < MX; k++) {
     const int j = jb + k;
     if (j < n) {
-      const double p = tab[R + j];
-      y[k] = tab[j] * buf[j];
+      const double p = PP(k);
+      y[k] = IB(k) * buf[j];
       B = fma(p, B, y[k]);
       A *= p;
     }
@@ -253,9 +209,8 @@ __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n,
   double d = carry_up(A, B, lane);
 #pragma unroll
   for (int k = 0; k < MX; k++) {
-    const int j = jb + k;
-    if (j < n) {
-      d = fma(tab[R + j], d, y[k]);
+    if (jb + k < n) {
+      d = fma(PP(k), d, y[k]);
       y[k] = d;
     }
   }
@@ -263,9 +218,8 @@ __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n,
   A = 1.0;
 #pragma unroll
   for (int k = MX - 1; k >= 0; k--) {
-    const int j = jb + k;
-    if (j < n) {
-      const double q = tab[2 * R + j];
+    if (jb + k < n) {
+      const double q = QQ(k);
       B = fma(q, B, y[k]);
       A *= q;
     }
@@ -275,107 +229,58 @@ __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n,
   for (int k = MX - 1; k >= 0; k--) {
     const int j = jb + k;
     if (j < n) {
-      x = fma(tab[2 * R + j], x, y[k]);
+      x = fma(QQ(k), x, y[k]);
       buf[j] = x;
     }
   }
 }
 
-// A line that crosses the interface: each lane recomputes the factors of its
-// rows from the stored bet of its first row (the factor recurrence of TDMA,
-// douglas_adi.cc:1790-1798): regular rows a, b, c of the node's side, the
-// Convert2Tri rows of the blocks, identity rows on the faces.
-template <int D, int MX>
-__device__ __forceinline__ void solve_cross(const Dev& P, double* buf, const FastChk& ck, int bend, int n, int lane) {
-  const int jb = lane * MX;
-  const MibBlock* __restrict__ blk = P.blk[D];
-  double y[MX], pk[MX], qk[MX];
-  double bet = ck.bet;
-  int side = ck.side;
-  int kb = ck.blk;
-  int Lk = kb < bend ? blk[kb].L : 0x7fffffff;
-  double B = 0.0, A = 1.0, qprev = 0.0;
-#pragma unroll
-  for (int k = 0; k < MX; k++) {
-    const int j = jb + k;
-    pk[k] = 0.0;
-    qk[k] = 0.0;
-    if (j < n) {
-      double a, b, c;
-      if (j == 0 || j == n - 1) {
-        a = 0.0;
-        b = 1.0;
-        c = 0.0;
-      } else if (j >= Lk) {
-        const MibBlock& bk = blk[kb];
-        const int q = j - Lk;
-        a = bk.ia[q];
-        b = bk.ib[q];
-        c = bk.ic[q];
-        if (q == bk.kind - 1) {
-          side = (bk.sides >> q) & 1;
-          kb++;
-          Lk = kb < bend ? blk[kb].L : 0x7fffffff;
-        }
-      } else {
-        a = P.ia[D][side];
-        b = P.ib[D][side];
-        c = P.ic[D][side];
-      }
-      if (k > 0) bet = fma(a, qprev, b);
-      const double ib = 1.0 / bet;
-      const double p = -a * ib;
-      qprev = -c * ib;
-      pk[k] = p;
-      qk[k] = qprev;
-      y[k] = ib * buf[j];
-      B = fma(p, B, y[k]);
-      A *= p;
-    }
-  }
-  double d = carry_up(A, B, lane);
-#pragma unroll
-  for (int k = 0; k < MX; k++) {
-    if (jb + k < n) {
-      d = fma(pk[k], d, y[k]);
-      y[k] = d;
-    }
-  }
-  B = 0.0;
-  A = 1.0;
-#pragma unroll
-  for (int k = MX - 1; k >= 0; k--) {
-    if (jb + k < n) {
-      B = fma(qk[k], B, y[k]);
-      A *= qk[k];
-    }
-  }
-  double x = carry_down(A, B, lane);
-#pragma unroll
-  for (int k = MX - 1; k >= 0; k--) {
-    const int j = jb + k;
-    if (j < n) {
-      x = fma(qk[k], x, y[k]);
-      buf[j] = x;
-    }
-  }
-}
-
-// Solve line lid of direction D held in buf (after its block rows).
-template <int D, int MX>
-__device__ __forceinline__ void solve_line(const Dev& P, double* buf, const double* stab, long long lid, int n,
-                                           int lane) {
+// A line without crossings: (ib, p, q) from the row table of its side in
+// shared memory, tab[0..R) = ib, tab[R..2R) = p, tab[2R..3R) = q.
+template <int MX>
+__device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n, int lane) {
   constexpr int R = 32 * MX;
-  const int bfirst = P.bstart[D][lid], bend = P.bstart[D][lid + 1];
-  if (bfirst == bend) {
-    const int side1 = (P.lside[D][lid] >> 1) & 1;
-    solve_tab<MX>(buf, stab + side1 * 3 * R, n, lane);
-  } else {
-    block_rows<D>(P, buf, bfirst, bend, lane);
-    __syncwarp();
-    const FastChk ck = P.fchk[D][lid * 32 + lane];
-    solve_cross<D, MX>(P, buf, ck, bend, n, lane);
+  const int jb = lane * MX;
+  solve_seg<MX>(
+      buf, n, lane, [&](int k) { return tab[jb + k]; }, [&](int k) { return tab[R + jb + k]; },
+      [&](int k) { return tab[2 * R + jb + k]; });
+}
+
+// A line that crosses the interface: the lane's rows of its own coefficients
+// (cf: [ib, p, q][R] in global memory, zero past the line end), loaded into
+// registers at once.
+template <int MX>
+struct LineCoef {
+  double ib[MX], p[MX], q[MX];
+  __device__ __forceinline__ void load(const double* __restrict__ cf, int lane) {
+    constexpr int R = 32 * MX;
+    const int jb = lane * MX;
+#pragma unroll
+    for (int k = 0; k < MX; k++) {
+      ib[k] = __ldg(cf + jb + k);
+      p[k] = __ldg(cf + R + jb + k);
+      q[k] = __ldg(cf + 2 * R + jb + k);
+    }
   }
+};
+template <int MX>
+__device__ __forceinline__ void solve_coef(double* buf, const LineCoef<MX>& c, int n, int lane) {
+  solve_seg<MX>(
+      buf, n, lane, [&](int k) { return c.ib[k]; }, [&](int k) { return c.p[k]; }, [&](int k) { return c.q[k]; });
+}
+
+// What a line's solve needs to know about it, loaded ahead of its data.
+struct LineMeta {
+  int bfirst, bend, side1, cidx;
+};
+template <int D>
+__device__ __forceinline__ LineMeta line_meta(const Dev& P, long long lid) {
+  LineMeta m;
+  m.bfirst = P.bstart[D][lid];
+  m.bend = P.bstart[D][lid + 1];
+  m.side1 = (P.lside[D][lid] >> 1) & 1;
+  m.cidx = P.fcidx[D] ? P.fcidx[D][lid] : -1;
+  return m;
 }
 
 // Row tables [side][ib, p, q][R] into shared memory.
@@ -384,200 +289,137 @@ __device__ __forceinline__ void load_tab(double* s, const double* g, int R) {
 }
 
 // ---------------------------------------------------------------------------
-// kf_x: rho fused with the x solves.
+// kf_mib: the MIB rows' right-hand sides of the x solve, into d.
 
-struct XLayout {
-  int slabd;  // doubles per u^n slab (TY+2 rows, aligned start, even)
-  int tagb;   // bytes per tag slab (TY rows, multiple of 16)
-  size_t o_tag, o_xt, o_tab, o_bar, total;
-};
-__host__ __device__ inline XLayout x_layout(int nx, int TY, int R) {
-  XLayout L;
-  L.slabd = ((TY + 2) * nx + 2 + 1) & ~1;
-  L.tagb = (TY * nx + 32 + 15) & ~15;
-  L.o_tag = (size_t)4 * L.slabd * sizeof(double);
-  L.o_xt = L.o_tag + (size_t)4 * L.tagb;
-  L.o_tab = L.o_xt + (((size_t)2 * nx * sizeof(double) + 15) & ~(size_t)15);
-  L.o_bar = L.o_tab + (size_t)6 * R * sizeof(double);
-  L.total = L.o_bar + 4 * sizeof(uint64_t);
-  return L;
+__global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                              double* __restrict__ d, double E) {
+  const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+  E = step_e(P, E, 2);
+  const int nxb = P.nblk[0];
+  if (t < nxb) {
+    // an x block: rho of its rows, then the Convert2Tri row operations
+    const MibBlock& b = P.blk[0][t];
+    const int iy = b.line / P.nz, iz = b.line % P.nz;
+    const long long m0 = (long long)P.nx * (iy + (long long)P.ny * iz);
+    double r[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < b.kind; q++) {
+      const long long m = m0 + b.L + q;
+      r[q] = rho_mib(P, un, E, m, b.L + q, iy, iz, P.tag[m]);
+    }
+    if (b.kind == 2) {
+      r[1] -= b.rate[0] * r[0];
+      r[0] -= b.rate[1] * r[1];
+    } else {
+      r[1] -= b.rate[0] * r[0];
+      r[2] -= b.rate[1] * r[0];
+      r[0] -= b.rate[2] * r[2];
+      r[1] -= b.rate[3] * r[2];
+      r[2] -= b.rate[4] * r[1];
+      r[0] -= b.rate[5] * r[1];
+    }
+    for (int q = 0; q < b.kind; q++) d[m0 + b.L + q] = r[q];
+    return;
+  }
+  const long long k = t - nxb;
+  if (k >= P.nmibnode) return;
+  const long long m = P.mibnode[k];
+  const int tg = P.tag[m];
+  if (tg & TAG_MIBX) return;  // its x block's thread writes it
+  int ix, iy, iz;
+  node_xyz(P, m, ix, iy, iz);
+  d[m] = rho_mib(P, un, E, m, ix, iy, iz, tg);
 }
 
-template <int TY, int MX>
-__global__ void __launch_bounds__(32 * TY, 2) kf_x(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                   double* __restrict__ dst, double E, int nyt, int zchunk,
-                                                   int ntiles) {
+// ---------------------------------------------------------------------------
+// kf_x: rho fused with the x solves.
+
+constexpr int XW = 8;  // warps per CTA of kf_x: a 4 (y) x 2 (z) block of lines
+
+template <int MX>
+__host__ __device__ constexpr size_t x_smem() {
+  // row tables 6 R, one line buffer of R doubles per warp
+  return sizeof(double) * ((size_t)6 * 32 * MX + (size_t)XW * 32 * MX);
+}
+
+template <int MX>
+__global__ void __launch_bounds__(32 * XW, 3) kf_x(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                   double* __restrict__ dst, double E) {
   constexpr int R = 32 * MX;
+  extern __shared__ __align__(16) double smx[];
+  double* const stab = smx;
+  load_tab(stab, P.ftab[0], R);
+  __syncthreads();
   E = step_e(P, E, 2);
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* const buf = smx + 6 * R + w * R;
   const bool eq8 = P.eq != 0;
-
-  if ((int)blockIdx.x >= ntiles) {
-    // face x lines (iy or iz on a face): d = Outer_u(t_next) - u^n
-    const int nface = 2 * ny + 2 * (nz - 2);
-    const int fw = (blockIdx.x - ntiles) * TY + w, fstride = (gridDim.x - ntiles) * TY;
-    for (int f = fw; f < nface; f += fstride) {
-      int iy, iz;
-      if (f < 2 * ny) {
-        iy = f % ny;
-        iz = f < ny ? 0 : nz - 1;
-      } else {
-        iz = 1 + (f - 2 * ny) % (nz - 2);
-        iy = (f - 2 * ny) < nz - 2 ? 0 : ny - 1;
-      }
-      const long long m0 = (long long)nx * (iy + (long long)ny * iz);
-      const double y = P.ax[1][iy], z = P.ax[2][iz];
-      const double yz2 = y * y + z * z;
-      for (int ix = lane; ix < nx; ix += 32) {
-        const double x = P.ax[0][ix];
-        const double out = eq8 ? (x * x + yz2) * E : 100.0;
-        dst[m0 + ix] = out - un[m0 + ix];
-      }
-    }
-    return;
-  }
-
-  extern __shared__ __align__(16) unsigned char smx[];
-  const XLayout LY = x_layout(nx, TY, R);
-  double* const slab = reinterpret_cast<double*>(smx);
-  unsigned char* const tslab = smx + LY.o_tag;
-  double* const xs2 = reinterpret_cast<double*>(smx + LY.o_xt);  // sin 2x
-  double* const xxx = xs2 + nx;                                   // x^2
-  double* const stab = reinterpret_cast<double*>(smx + LY.o_tab);
-  uint64_t* const bar = reinterpret_cast<uint64_t*>(smx + LY.o_bar);
-
-  const int ty = blockIdx.x % nyt, zc = blockIdx.x / nyt;
-  const int y0 = 1 + ty * TY;
-  const int z0 = 1 + zc * zchunk;
-  const int z1 = min(z0 + zchunk, nz - 1);
-  const int nplanes = z1 - z0;  // >= 1
-  const int nslabs = nplanes + 2;
-
-  // slab i holds plane z0 - 1 + i: where each copy starts, and the offset
-  // (in elements) of the data within the aligned copy
-  auto slab_src = [&](int i, int& shift) -> const double* {
-    const double* g = un + (long long)nx * ((y0 - 1) + (long long)ny * (z0 - 1 + i));
-    const uintptr_t a = reinterpret_cast<uintptr_t>(g);
-    shift = (int)((a & 15) >> 3);
-    return reinterpret_cast<const double*>(a & ~(uintptr_t)15);
-  };
-  auto tag_src = [&](int i, int& shift) -> const unsigned char* {
-    const unsigned char* g = P.tag + (long long)nx * (y0 + (long long)ny * (z0 - 1 + i));
-    const uintptr_t a = reinterpret_cast<uintptr_t>(g);
-    shift = (int)(a & 15);
-    return reinterpret_cast<const unsigned char*>(a & ~(uintptr_t)15);
-  };
-  const unsigned ubytes = (unsigned)((((size_t)(TY + 2) * nx + 1) * sizeof(double) + 15) & ~(size_t)15);
-  const unsigned tbytes = (unsigned)((TY * nx + 15 + 15) & ~15);
-  auto issue = [&](int i) {
-    const int s = i & 3;
-    int sh;
-    const double* gu = slab_src(i, sh);
-    const unsigned char* gt = tag_src(i, sh);
-    mbar_expect(&bar[s], ubytes + tbytes);
-    bulk_copy(slab + (size_t)s * LY.slabd, gu, ubytes, &bar[s]);
-    bulk_copy(tslab + (size_t)s * LY.tagb, gt, tbytes, &bar[s]);
-  };
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < 4; s++) mbar_init(&bar[s]);
-    mbar_init_fence();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int i = 0; i < 3 && i < nslabs; i++) issue(i);
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    xs2[i] = P.s2[0][i];
-    const double x = P.ax[0][i];
-    xxx[i] = x * x;
-  }
-  load_tab(stab, P.ftab[0], R);
-  __syncthreads();
-
+  const long long sy = nx, sz = (long long)nx * ny;
   // dt beta / h^2 of each direction, by side
   const double cx0 = P.dt * P.vd[0][0][0], cy0 = P.dt * P.vd[1][0][0], cz0 = P.dt * P.vd[2][0][0];
   const double cx1 = P.dt * P.vd[0][1][0], cy1 = P.dt * P.vd[1][1][0], cz1 = P.dt * P.vd[2][1][0];
-  const int iy = y0 + w;
-  const bool live = iy <= ny - 2;
-  const double yv = P.ax[1][live ? iy : 1];
-  const int jb = lane * MX;
-  bool bad = false;
-
-  for (int pi = 0; pi < nplanes; pi++) {
-    if (threadIdx.x == 0 && pi + 3 < nslabs) issue(pi + 3);
-    const int iz = z0 + pi;
-    // slabs pi (z-1), pi+1 (z), pi+2 (z+1) must have landed
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const int i = pi + k;
-      ok = ok && mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
+  const int nbY = (ny + 3) / 4, nbZ = (nz + 1) / 2;
+  const long long nb = (long long)nbY * nbZ;
+  for (long long blk = blockIdx.x; blk < nb; blk += gridDim.x) {
+    const int iy = (int)(blk % nbY) * 4 + (w & 3), iz = (int)(blk / nbY) * 2 + (w >> 2);
+    if (iy >= ny || iz >= nz) continue;  // (warp-uniform)
+    const long long m0 = (long long)nx * (iy + (long long)ny * iz);
+    const double yv = P.ax[1][iy], zv = P.ax[2][iz];
+    const double yz2 = yv * yv + zv * zv;
+    if (iy == 0 || iz == 0 || iy == ny - 1 || iz == nz - 1) {
+      // face line: d = Outer_u(t_next) - u^n
+      for (int j = lane; j < nx; j += 32) {
+        const double x = P.ax[0][j];
+        dst[m0 + j] = (eq8 ? (x * x + yz2) * E : 100.0) - un[m0 + j];
+      }
+      continue;
     }
-    if (!ok) bad = true;
-    if (live && ok) {
-      int shm, shc, shp, tsh;
-      slab_src(pi, shm);
-      slab_src(pi + 1, shc);
-      slab_src(pi + 2, shp);
-      tag_src(pi + 1, tsh);
-      const double* const sc = slab + (size_t)((pi + 1) & 3) * LY.slabd + shc + (size_t)(w + 1) * nx;
-      const double* const sym = sc - nx;
-      const double* const syp = sc + nx;
-      double* const szm = slab + (size_t)(pi & 3) * LY.slabd + shm + (size_t)(w + 1) * nx;
-      const double* const szp = slab + (size_t)((pi + 2) & 3) * LY.slabd + shp + (size_t)(w + 1) * nx;
-      const unsigned char* const tg = tslab + (size_t)((pi + 1) & 3) * LY.tagb + tsh + (size_t)w * nx;
-      const double zv = P.ax[2][iz];
-      const double yz2 = yv * yv + zv * zv;
-      // source constants of the line: inside dt kin sin2x cos2y sin2z E,
-      // outside -dt E (x^2 + y^2 + z^2) - dt 6 beta_out E
-      const double kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
-      const double koa = eq8 ? -P.dt * E : 0.0;
-      const double kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
-      const long long m0 = (long long)nx * (iy + (long long)ny * iz);
-      // rho into the line buffer: the z-1 row of this line, which no other
-      // warp reads (each element is read before this lane overwrites it)
-      double* const buf = szm;
-#pragma unroll
-      for (int k = 0; k < MX; k++) {
-        const int j = jb + k;
-        if (j < nx) {
-          const double uc = sc[j];
-          double r;
-          if (j == 0 || j == nx - 1) {
-            r = (eq8 ? fma(xxx[j], E, yz2 * E) : 100.0) - uc;
-          } else {
-            const int t = tg[j];
-            if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
-              r = rho_mib(P, un, E, m0 + j, j, iy, iz, t);
-            } else {
-              const double lx = fma(-2.0, uc, sc[j - 1] + sc[j + 1]);
-              const double ly = fma(-2.0, uc, sym[j] + syp[j]);
-              const double lz = fma(-2.0, uc, buf[j] + szp[j]);
-              if (t & TAG_OUT)
-                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, xxx[j], kob))));
-              else
-                r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * xs2[j])));
-            }
-          }
-          buf[j] = r;
+    const long long lid = (long long)iy * nz + iz;
+    const LineMeta lm = line_meta<0>(P, lid);
+    // source constants of the line: inside dt kin sin2x cos2y sin2z E,
+    // outside -dt E (x^2 + y^2 + z^2) - dt 6 beta_out E
+    const double kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
+    const double koa = eq8 ? -P.dt * E : 0.0;
+    const double kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
+    const double* const ur = un + m0;
+    const unsigned char* const tr = P.tag + m0;
+#pragma unroll 3
+    for (int k = 0; k < MX; k++) {
+      const int j = lane + 32 * k;
+      if (j < nx) {
+        // (an interior line: every neighbour index lies inside the field)
+        const int t = tr[j];
+        const double uc = ur[j], uxm = ur[j - 1], uxp = ur[j + 1];
+        const double uym = ur[j - sy], uyp = ur[j + sy], uzm = ur[j - sz], uzp = ur[j + sz];
+        const double x = P.ax[0][j], s2x = P.s2[0][j];
+        double r;
+        if (j == 0 || j == nx - 1) {
+          r = (eq8 ? fma(x * x, E, yz2 * E) : 100.0) - uc;
+        } else if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
+          r = dst[m0 + j];  // from kf_mib
+        } else {
+          const double lx = fma(-2.0, uc, uxm + uxp);
+          const double ly = fma(-2.0, uc, uym + uyp);
+          const double lz = fma(-2.0, uc, uzm + uzp);
+          if (t & TAG_OUT)
+            r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, x * x, kob))));
+          else
+            r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * s2x)));
         }
+        buf[j] = r;
       }
-      __syncwarp();
-      solve_line<0, MX>(P, buf, stab, (long long)iy * nz + iz, nx, lane);
-      __syncwarp();
-      for (int j = lane; j < nx; j += 32) dst[m0 + j] = buf[j];
     }
-    // every thread's shared-memory accesses to the slot reloaded next are done
-    fence_async_smem();
-    if (__syncthreads_or(bad)) {
-      if (threadIdx.x == 0) {
-        atomicOr(P.status, 2);
-        // let the copies still in flight land before the CTA leaves
-        for (int i = pi + 3; i < nslabs && i < pi + 4; i++) mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
-      }
-      return;
+    __syncwarp();
+    if (lm.bend > lm.bfirst) {
+      LineCoef<MX> c;
+      c.load(P.fcoef[0] + (size_t)lm.cidx * 3 * R, lane);
+      solve_coef<MX>(buf, c, nx, lane);
+    } else {
+      solve_tab<MX>(buf, stab + lm.side1 * 3 * R, nx, lane);
     }
+    __syncwarp();
+    for (int j = lane; j < nx; j += 32) dst[m0 + j] = buf[j];
+    __syncwarp();  // the buffer is free for the next line
   }
 }
 
@@ -647,14 +489,25 @@ __global__ void __launch_bounds__(32 * YZ_NL, 3) kf_yz(const __grid_constant__ D
     const Tile nxt = tile_of(t + gridDim.x);
     double* const buf = bufs + (size_t)(it & 1) * YZ_NL * LS;
     copy_in(nxt, bufs + (size_t)((it + 1) & 1) * YZ_NL * LS);
+    // warp w's line of this tile: what its solve needs, loaded before the
+    // tile's data has landed
+    const int i1w = cur.i1 + w;
+    const bool solve = i1w < i1lo + i1n && i1w >= 1 && i1w <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
+    LineMeta lm{0, 0, 0, -1};
+    const long long lid = (long long)i1w * n2 + cur.i2;
+    if (solve) lm = line_meta<D>(P, lid);
     cp_async_wait<1>();
     __syncthreads();
-    {
-      const int i1 = cur.i1 + w;
-      const bool interior = i1 >= 1 && i1 <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
-      if (i1 < i1lo + i1n && interior) {
-        const long long lid = (long long)i1 * n2 + cur.i2;
-        solve_line<D, MX>(P, buf + w * LS, stab, lid, n, lane);
+    if (solve) {
+      double* const lb = buf + w * LS;
+      if (lm.bend > lm.bfirst) {
+        LineCoef<MX> cf;
+        cf.load(P.fcoef[D] + (size_t)lm.cidx * 3 * R, lane);
+        block_rows<D>(P, lb, lm.bfirst, lm.bend, lane);
+        __syncwarp();
+        solve_coef<MX>(lb, cf, n, lane);
+      } else {
+        solve_tab<MX>(lb, stab + lm.side1 * 3 * R, n, lane);
       }
     }
     __syncthreads();
@@ -709,45 +562,53 @@ __global__ void __launch_bounds__(TPB) kf_tab(const __grid_constant__ Dev P, dou
   T[2 * R + j] = q;
 }
 
-// Checkpoints of the lines that cross the interface: for lane l, the bet of
-// row l MX (the prefix table before the first MIB row, the per-node factors
-// from it on), the side of the regular rows there and the first block that
-// ends at or after it.
+// Coefficients of the lines that cross the interface, one thread per line,
+// walking the line as the sequential sweep does (the factors from the prefix
+// table before the first MIB row and per node from it on; the regular rows'
+// side from the line's start and after each block), into the line's slot c
+// of cf: [c][ib, p, q][R].
 template <int D>
-__global__ void __launch_bounds__(TPB) kf_chk(const __grid_constant__ Dev P, FastChk* chk, int MX) {
+__global__ void __launch_bounds__(TPB) kf_coef(const __grid_constant__ Dev P, double* cf, int R) {
   const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
-  const long long line = t >> 5;
-  const int l = (int)(t & 31);
-  if (line >= nlines<D>(P)) return;
+  if (t >= nlines<D>(P)) return;
   Line L;
-  decode_line<D>(P, line, L);
+  decode_line<D>(P, t, L);
   if (L.boundary) return;
   const int bfirst = P.bstart[D][L.lid], bend = P.bstart[D][L.lid + 1];
   if (bfirst == bend) return;
-  const int jb = l * MX;
-  if (jb >= L.n) return;
-  const MibBlock* blk = P.blk[D];
+  const int n = L.n;
+  const long long s = L.s;
+  const MibBlock* const blk = P.blk[D];
   const int L1 = blk[bfirst].L;
   const int side1 = (P.lside[D][L.lid] >> 1) & 1;
-  FastChk c;
-  c.bet = jb < L1 ? P.ptab[D][side1][2 * jb] : P.fbet[D][L.base + (long long)jb * L.s];
-  int side = side1, k = bfirst;
-  while (k < bend && blk[k].L + blk[k].kind - 1 < jb) {
-    side = (blk[k].sides >> (blk[k].kind - 1)) & 1;
-    k++;
+  const double* const pt = P.ptab[D][side1];
+  double* const c = cf + (size_t)P.fcidx[D][L.lid] * 3 * R;
+  int b = bfirst, side = side1;
+  for (int j = 0; j < n; j++) {
+    const long long g = L.base + (long long)j * s;
+    const double bet = j >= L1 ? P.fbet[D][g] : pt[2 * j];
+    double a;
+    if (j == 0 || j == n - 1) {
+      a = 0.0;
+    } else if (b < bend && j >= blk[b].L) {
+      const int q = j - blk[b].L;
+      a = blk[b].ia[q];
+      if (q == blk[b].kind - 1) {
+        side = (blk[b].sides >> q) & 1;
+        b++;
+      }
+    } else {
+      a = P.ia[D][side];
+    }
+    const double gn = j == n - 1 ? 0.0 : j + 1 >= L1 ? P.fgam[D][g + s] : pt[2 * (j + 1) + 1];
+    c[j] = 1.0 / bet;
+    c[R + j] = -(a / bet);
+    c[2 * R + j] = -gn;
   }
-  c.side = side;
-  c.blk = k;
-  chk[(long long)L.lid * 32 + l] = c;
 }
 
 // ---------------------------------------------------------------------------
 // Launch shapes
-
-template <int TY, int MX>
-size_t x_smem_of(int nx) {
-  return x_layout(nx, TY, 32 * MX).total;
-}
 
 int fast_mx(int n) {
   const int c[6] = {1, 3, 5, 9, 13, 17};
@@ -756,29 +617,14 @@ int fast_mx(int n) {
   return 0;
 }
 
-// kf_x with TY lines per CTA: the z range of a CTA is chosen so that the
-// tiles fill the resident CTAs of the GPU about once.
-template <int TY, int MX>
-void launch_x(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  const size_t smem = x_smem_of<TY, MX>(P.nx);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_x<TY, MX>, 32 * TY, smem);
-  if (per_sm < 1) per_sm = 1;
-  const int nyt = (P.ny - 2 + TY - 1) / TY;
-  const int target = std::max(1, per_sm * P.sweep_blocks - X_NFACE);
-  int nzc = std::max(1, std::min(P.nz - 2, target / nyt));
-  const int zchunk = (P.nz - 2 + nzc - 1) / nzc;
-  nzc = (P.nz - 2 + zchunk - 1) / zchunk;
-  const int ntiles = nyt * nzc;
-  kf_x<TY, MX><<<ntiles + X_NFACE, 32 * TY, smem, st>>>(P, un, d, E, nyt, zchunk, ntiles);
-}
-
 template <int MX>
-void launch_x_mx(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  if (x_smem_of<8, MX>(P.nx) <= (size_t)113 * 1024)
-    launch_x<8, MX>(P, un, d, E, st);
-  else
-    launch_x<4, MX>(P, un, d, E, st);
+void launch_x(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_x<MX>, 32 * XW, x_smem<MX>());
+  if (per_sm < 1) per_sm = 1;
+  const long long nb = (long long)((P.ny + 3) / 4) * ((P.nz + 1) / 2);
+  const int grid = (int)std::max(1LL, std::min(nb, (long long)per_sm * P.sweep_blocks));
+  kf_x<MX><<<grid, 32 * XW, x_smem<MX>(), st>>>(P, un, d, E);
 }
 
 template <int D, int MX, bool ACC>
@@ -813,21 +659,16 @@ void launch_x_n(const Dev& P, const double* un, double* d, double E, cudaStream_
   switch (fast_mx(P.nx)) {
 #define MTS_CASE(mx) \
   case mx:           \
-    launch_x_mx<mx>(P, un, d, E, st); \
+    launch_x<mx>(P, un, d, E, st); \
     break;
     MTS_FAST_MX(MTS_CASE)
 #undef MTS_CASE
   }
 }
 
-template <int TY, int MX>
-void x_attr() {
-  cudaFuncSetAttribute(kf_x<TY, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSweepSmem);
-}
 template <int MX>
 void fast_attr() {
-  x_attr<8, MX>();
-  x_attr<4, MX>();
+  cudaFuncSetAttribute(kf_x<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x_smem<MX>());
   cudaFuncSetAttribute(kf_yz<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yz_smem<MX>());
   cudaFuncSetAttribute(kf_yz<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yz_smem<MX>());
 }
@@ -844,9 +685,7 @@ int fast_rows_per_lane(int n) { return fast_mx(n); }
 
 bool fast_fits(int nx, int ny, int nz) {
   const int mx = fast_mx(nx), my = fast_mx(ny), mz = fast_mx(nz);
-  if (!mx || !my || !mz) return false;
-  if (x_layout(nx, 4, 32 * mx).total > (size_t)kMaxSweepSmem) return false;
-  return true;
+  return mx && my && mz;
 }
 
 int build_fast_tables(const Dev& P, cudaStream_t st) {
@@ -861,11 +700,10 @@ int build_fast_tables(const Dev& P, cudaStream_t st) {
     if (d == 2) kf_tab<2><<<g, TPB, 0, st>>>(P, tab, R);
     launches++;
     if (P.nblk[d] == 0) continue;
-    FastChk* chk = const_cast<FastChk*>(P.fchk[d]);
-    const int mx = fast_mx(nd[d]);
-    if (d == 0) kf_chk<0><<<(unsigned)((nlines<0>(P) * 32 + TPB - 1) / TPB), TPB, 0, st>>>(P, chk, mx);
-    if (d == 1) kf_chk<1><<<(unsigned)((nlines<1>(P) * 32 + TPB - 1) / TPB), TPB, 0, st>>>(P, chk, mx);
-    if (d == 2) kf_chk<2><<<(unsigned)((nlines<2>(P) * 32 + TPB - 1) / TPB), TPB, 0, st>>>(P, chk, mx);
+    double* cf = const_cast<double*>(P.fcoef[d]);
+    if (d == 0) kf_coef<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
+    if (d == 1) kf_coef<1><<<(unsigned)((nlines<1>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
+    if (d == 2) kf_coef<2><<<(unsigned)((nlines<2>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
     launches++;
   }
   return launches;
@@ -875,7 +713,13 @@ int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cud
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[k], st);
   };
+  int launches = 3;
   mark(0);
+  if (P.nblk[0] > 0 || P.nmibnode > 0) {
+    const long long nt = (long long)P.nblk[0] + P.nmibnode;
+    kf_mib<<<(unsigned)((nt + TPB - 1) / TPB), TPB, 0, st>>>(P, u, d, T.e_next);
+    launches++;
+  }
   launch_x_n(P, u, d, T.e_next, st);
   mark(1);
   mark(2);
@@ -884,7 +728,7 @@ int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cud
   mark(4);
   launch_yz_n<2, true>(P, d, u, st);
   mark(5);
-  return 3;
+  return launches;
 }
 
 }  // namespace mts
