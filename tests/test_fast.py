@@ -7,7 +7,8 @@ fused multiply-adds, and each line is solved by one warp in segments joined
 by shuffle scans), so it matches the reference up to rounding only.
 Tolerance, the plain form's contract: 1e-10 relative max-norm
 (max |u_fast - u_ref| / max |u_ref|).  The L-infinity and L2 errors against
-the exact solution must agree with the reference's to 1e-8 relative."""
+the exact solution must agree with the reference's to 1e-8 relative (plus
+1e-11 absolute, for the Eq_0 case whose errors are rounding alone)."""
 import numpy as np
 import pytest
 
@@ -37,7 +38,9 @@ def run(spec, steps, precision="fast", tags=None, crossings=None, u0=None):
 
 
 def close_norms(a, b):
-    return abs(a - b) <= NORM_TOL * max(abs(b), 1e-300)
+    # (plus 1e-11 absolute: the Eq_0 known answer has errors of ~1e-13 that
+    # are rounding alone)
+    return abs(a - b) <= NORM_TOL * abs(b) + 1e-11
 
 
 @pytest.mark.parametrize("path", ["own_setup", "reference_crossings"])
