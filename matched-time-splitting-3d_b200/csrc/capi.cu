@@ -631,7 +631,7 @@ mts_status enqueue_step(mts_problem* h, double t_prev, double t_half, double t_n
   }
   CUDA_TRY(ensure_side_stream(h));
   if (h->dev.precision == 2)
-    h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, ev);
+    h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, ev, &h->side);
   else if (h->dev.precision == 1)
     h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, ev, &h->side);
   else
@@ -941,7 +941,7 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     for (int k = 0; k < counts[i]; k++) {
       mts::StepTimes T{0, 0, 0};  // unused: the kernels read the table
       if (h->dev.precision == 2)
-        h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, nullptr);
+        h->launches += mts::launch_step_fast(h->dev, T, h->u0, h->u1, h->stream, nullptr, &h->side);
       else if (h->dev.precision == 1)
         h->launches += mts::launch_step_mixed(h->dev, T, h->u0, h->stream, nullptr, &h->side);
       else
@@ -1158,35 +1158,55 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
     if (!mts::fast_fits(h->g.nx, h->g.ny, h->g.nz))
       return fail(MTS_ERR_ARG, "grid lines too long for the fast FP64 form (at most 544 nodes per axis)");
     if (!h->dev.ftab[0]) {
-      // row tables, and the coefficients of the lines that cross the
-      // interface (numbered in line order), once per handle
+      // row tables, line flags, the crossing lines' list and coefficients,
+      // the block rows' q and the MIB nodes' block references, once per
+      // handle
+      mts::Dev& D = h->dev;
       const int nd[3] = {h->g.nx, h->g.ny, h->g.nz};
+      uint8_t* fl[3] = {nullptr, nullptr, nullptr};
       for (int d = 0; d < 3; d++) {
         const size_t R = 32 * (size_t)mts::fast_rows_per_lane(nd[d]);
         double* tab = nullptr;
-        CUDA_TRY(h->put(&tab, (const double*)nullptr, 6 * R));
-        h->dev.ftab[d] = tab;
-        h->dev.fcoef[d] = nullptr;
-        h->dev.fcidx[d] = nullptr;
-        if (h->nblk[d] == 0) continue;
+        CUDA_TRY(h->put(&tab, (const double*)nullptr, 4 * R));
+        D.ftab[d] = tab;
+        CUDA_TRY(h->put(&fl[d], (const uint8_t*)nullptr, (size_t)line_count(h->g, d)));
+        D.fline[d] = fl[d];
+      }
+      mts::build_fast_lines(D, fl, h->stream);
+      CUDA_TRY(cudaGetLastError());
+      for (int d = 0; d < 3; d++) {
+        const size_t R = 32 * (size_t)mts::fast_rows_per_lane(nd[d]);
         const size_t nl = (size_t)line_count(h->g, d);
-        std::vector<int32_t> bs(nl + 1), cidx(nl, -1);
-        CUDA_TRY(cudaMemcpyAsync(bs.data(), h->dev.bstart[d], bs.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                 h->stream));
+        std::vector<uint8_t> hf(nl);
+        CUDA_TRY(cudaMemcpyAsync(hf.data(), fl[d], nl, cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
-        int32_t nc = 0;
+        std::vector<int32_t> list;
         for (size_t l = 0; l < nl; l++)
-          if (bs[l + 1] > bs[l]) cidx[l] = nc++;
-        int32_t* dci = nullptr;
-        CUDA_TRY(h->put(&dci, cidx.data(), nl));
-        double* cf = nullptr;
-        CUDA_TRY(h->put(&cf, (const double*)nullptr, 3 * R * (size_t)nc));
-        CUDA_TRY(cudaMemsetAsync(cf, 0, 3 * R * (size_t)nc * sizeof(double), h->stream));
-        h->dev.fcidx[d] = dci;
-        h->dev.fcoef[d] = cf;
-        // the host vector must outlive the asynchronous upload
+          if (hf[l] & 1) list.push_back((int32_t)l);
+        int32_t* dl = nullptr;
+        double *cf = nullptr, *bq = nullptr;
+        if (!list.empty()) {
+          CUDA_TRY(h->put(&dl, list.data(), list.size()));
+          CUDA_TRY(h->put(&cf, (const double*)nullptr, 2 * R * list.size()));
+          CUDA_TRY(cudaMemsetAsync(cf, 0, 2 * R * list.size() * sizeof(double), h->stream));
+        }
+        if (h->nblk[d] > 0) CUDA_TRY(h->put(&bq, (const double*)nullptr, 3 * (size_t)h->nblk[d]));
+        D.fcross[d] = dl;
+        D.nfcross[d] = (int)list.size();
+        D.fcoef[d] = cf;
+        D.fbq[d] = bq;
+        // the host list must outlive the asynchronous upload
         CUDA_TRY(cudaStreamSynchronize(h->stream));
       }
+      int4* ref = nullptr;
+      int32_t* xb = nullptr;
+      if (D.nmibnode > 0) CUDA_TRY(h->put(&ref, (const int4*)nullptr, (size_t)D.nmibnode));
+      if (h->nblk[0] > 0) {
+        CUDA_TRY(h->put(&xb, (const int32_t*)nullptr, 3 * (size_t)h->nblk[0]));
+        CUDA_TRY(cudaMemsetAsync(xb, 0, 3 * (size_t)h->nblk[0] * sizeof(int32_t), h->stream));
+      }
+      D.mibref = ref;
+      D.xbmib = xb;
       mts::build_fast_tables(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(cudaStreamSynchronize(h->stream));

@@ -122,13 +122,21 @@ struct Dev {
   float* ctab[3];
   int precision;              // 0 plain FP64, 1 mixed, 2 fast FP64
   // Fast FP64 form (segmented line solves, fast.cu), built when the form is
-  // switched on: per direction, the row tables [side][1/bet, -a/bet,
-  // -gam_{j+1}][32 MX] of the lines without crossings, and the same three
-  // values per row for each line that crosses the interface,
-  // fcoef[c][3][32 MX], c = fcidx[line] (-1 for the other lines).
+  // switched on.  Per direction: the row tables [side][1/bet, -a/bet][32 MX]
+  // of the lines without crossings; per line a flag byte (bit0 the line
+  // crosses the interface, bit1 the side of its row 1); the crossing lines'
+  // ids in line order (fcross, nfcross of them) and their own rows
+  // [c][1/bet, -a/bet][32 MX]; per block the -gam_{j+1} of its rows.  Per
+  // MIB node its block in x, y, z (-1: none); per x block the MIB node
+  // index of each of its rows.
   const double* ftab[3];
+  const uint8_t* fline[3];
+  const int32_t* fcross[3];
+  int nfcross[3];
   const double* fcoef[3];
-  const int32_t* fcidx[3];
+  const double* fbq[3];
+  const int4* mibref;
+  const int32_t* xbmib;
   // Replayable steps (batches captured in a CUDA graph): when tsched is set,
   // kernels take the step's exp(-t) factors from tsched[3*(*tstep) + {0: t_prev,
   // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
@@ -181,11 +189,13 @@ int build_mixed_coefs(const Dev& P, cudaStream_t stream);
 // The fast FP64 Douglas-ADI step (fast.cu): u holds u^n on entry and
 // u^{n+1} on return, d is scratch.  ev: null, or 6 events recorded around
 // the three launches.
-int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cudaStream_t stream, cudaEvent_t* ev);
+int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cudaStream_t stream, cudaEvent_t* ev,
+                     const SideStream* side);
 void configure_fast_kernels();
 int fast_rows_per_lane(int n);               // MX of a direction with n rows (0: lines too long)
 bool fast_fits(int nx, int ny, int nz);      // the form takes this grid
-int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab / fcoef (allocated by the caller)
+int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t stream);  // the line flags
+int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab, fcoef, fbq, mibref, xbmib (allocated by the caller)
 // Batched plain steps (kernels.cu): problems of one method advance together,
 // one launch per kernel of the step for all of them.  A launch's CTAs are
 // listed as items (problem, the CTA's index in that problem's own grid, the

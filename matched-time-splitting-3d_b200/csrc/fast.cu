@@ -8,38 +8,44 @@
 // with d = Outer_u(t^{n+1}) - u^n on the faces (A_d = dt beta D_dd with the
 // MIB rows, src = f plus the jump terms of Src_2nd, douglas_adi.cc:1123-1428).
 // Everything here is FP64; the result differs from the reference's sequence
-// of operations only by rounding.  A step is four launches:
+// of operations only by rounding.
 //
-//   kf_mib the right-hand side of every MIB row (the explicit MIB sums of all
-//          three directions and the jump terms, one thread per node; the
-//          Convert2Tri row operations of the x blocks, one thread per
-//          block), written into the d field at those nodes.  Their
-//          dependent table walks run here, spread over many threads, and not
-//          inside the line solves.
-//   kf_x   rho fused with the x line solves: warp w of a CTA takes one x
-//          line at a time (the CTA's warps take a 4 x 2 block of lines, so
-//          that a line's y and z neighbours are mostly its siblings' lines
-//          and come from L1), forms rho of its rows from coalesced loads of
-//          u^n (taking the MIB rows from kf_mib), solves the line in shared
-//          memory and writes d*.
-//   kf_yz  the y solve in place on d*, and the z solve with the accumulation
-//          u^{n+1} = u^n + d.  A CTA copies NL neighbouring lines (the same
-//          row of NL lines is NL consecutive doubles) into shared memory,
-//          double-buffered so that the next tile's copy overlaps this tile's
-//          solves, and warp w solves line w (the Convert2Tri row operations
-//          of its blocks first, douglas_adi.cc:1554-1675).
+// Lines are split by kind.  Most lines do not cross the interface: their
+// Thomas factors are those of a line of one side, from a per-side row table,
+// and their kernels carry no dependent memory reads.  The lines that cross
+// the interface (a few tens of percent at most) have their own factors and
+// MIB blocks; they are solved by separate kernels on a second stream, at the
+// same time as the others.  A step is:
+//
+//   kf_mib  the right-hand side of every MIB row (the explicit MIB sums of
+//           all three directions and the jump terms, one thread per node;
+//           the Convert2Tri row operations of the x blocks, one thread per
+//           block, douglas_adi.cc:1554-1675), written into d at those nodes;
+//   kf_xr   rho of the regular x lines (and d on the face lines), fused with
+//           their solves: warp w of a CTA takes one line at a time, the CTA's
+//           warps a 4 (y) x 2 (z) block of lines, so that a line's y and z
+//           neighbours are mostly its siblings' lines and come from L1;
+//   kf_xc   the same for the x lines that cross the interface (side stream);
+//   kf_yt   the regular y lines, solved in place on d*, in tiles of NL
+//           neighbouring lines (the same row of NL lines is NL consecutive
+//           doubles) copied into shared memory with cp.async, double-buffered
+//           so that the next tile's copy overlaps this tile's solves;
+//   kf_yc   the y lines that cross the interface, one warp per line, their
+//           Convert2Tri row operations first (side stream);
+//   kf_yt / kf_yc for z, with the update u^{n+1} = u^n + d (u^n of a tile
+//           is copied in while the tile is solved).
 //
 // Line solve: with the Thomas factors fixed (bet_j, gam_j of TDMA,
 // douglas_adi.cc:1784-1807), both recurrences are first-order and linear:
 //   forward   d_j = (r_j - a_j d_{j-1}) / bet_j = ib_j r_j + p_j d_{j-1}
 //   backward  x_j = d_j - gam_{j+1} x_{j+1}    = d_j + q_j x_{j+1}
-// with ib = 1/bet, p = -a/bet, q = -gam_{j+1}.  Lane l of the warp takes the
-// rows [l MX, l MX + MX); each lane runs its rows from a zero carry, the
-// lanes' affine end maps are composed by a shuffle scan, and a second pass
-// runs the rows again from the true carry.  Lines without crossings read
-// (ib, p, q) from per-side row tables in shared memory; the lines that cross
-// the interface read their own, stored line after line ([line][ib, p, q][row]),
-// so that each lane loads its rows' 27 values in one round.
+// with ib = 1/bet, p = -a/bet, q = -gam_{j+1} = -c_j/bet_j.  On every row
+// that is not a MIB block row, a = c (the weights beta/h^2 on both sides of a
+// node are the same number), so q = p exactly: the tables and the crossing
+// lines' coefficients hold (ib, p) per row, and only block rows carry their
+// own q.  Lane l of the warp takes the rows [l MX, l MX + MX); each lane runs
+// its rows from a zero carry, the lanes' affine end maps are composed by a
+// shuffle scan, and a second pass runs the rows again from the true carry.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,7 +57,9 @@ namespace mts {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int YZ_NL = 8;     // lines per tile of kf_yz (one warp each)
+constexpr int YZ_NL = 8;  // lines per tile of kf_yt (one warp each)
+constexpr int XW = 8;     // warps per CTA of kf_xr: a 4 (y) x 2 (z) block of lines
+constexpr int CW = 8;     // warps per CTA of the crossing-line kernels
 
 // ---------------------------------------------------------------------------
 // Jump data on the fly (Refresh_Jump, intersection.cc:2294-2490): [u] and
@@ -89,70 +97,78 @@ __device__ __forceinline__ double src_jumps(const Dev& P, double E, double src, 
   return src + vd[0] * corner_jumps(b.w[2], Jl, Jr);
 }
 
-// rho at a node that is a MIB row of some x, y or z block: the explicit MIB
-// sums of douglas_adi.cc:112-210 (no jumps) and the jump terms of Src_2nd.
+// rho at a MIB node m = (ix, iy, iz): the explicit MIB sums of
+// douglas_adi.cc:112-210 (no jumps) in every direction the node is a block
+// row of, the regular three-point sums in the others, and the jump terms of
+// Src_2nd.  ref: the node's block in x, y, z (-1: none).
 __device__ __noinline__ double rho_mib(const Dev& P, const double* __restrict__ un, double E, long long m, int ix,
-                                       int iy, int iz, int tg) {
+                                       int iy, int iz, int tg, int4 ref) {
   const int side = tg & TAG_OUT;
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const double* vdx = P.vd[0][side];
   const double* vdy = P.vd[1][side];
   const double* vdz = P.vd[2][side];
-  int xr = 0, yr = 0, zr = 0;
-  const MibBlock* xb = (tg & TAG_MIBX) ? find_block<0>(P, iy * P.nz + iz, ix, xr) : nullptr;
-  const MibBlock* yb = (tg & TAG_MIBY) ? find_block<1>(P, ix * P.nz + iz, iy, yr) : nullptr;
-  const MibBlock* zb = (tg & TAG_MIBZ) ? find_block<2>(P, ix * P.ny + iy, iz, zr) : nullptr;
+  const MibBlock* xb = ref.x >= 0 ? &P.blk[0][ref.x] : nullptr;
+  const MibBlock* yb = ref.y >= 0 ? &P.blk[1][ref.y] : nullptr;
+  const MibBlock* zb = ref.z >= 0 ? &P.blk[2][ref.z] : nullptr;
   double sx, sy_, sz_;
   if (xb) {
     const long long base = m - ix;
-    sx = mib_sum(*xb, xr, [&](int j) { return un[base + j]; }, vdx, false, P.jv);
+    sx = mib_sum(*xb, ix - xb->L, [&](int j) { return un[base + j]; }, vdx, false, P.jv);
   } else {
     sx = (un[m - 1] * vdx[0] + un[m] * vdx[1]) + un[m + 1] * vdx[2];
   }
   if (yb) {
     const long long base = ix + sz * iz;
-    sy_ = mib_sum(*yb, yr, [&](int j) { return un[base + (long long)j * sy]; }, vdy, false, P.jv);
+    sy_ = mib_sum(*yb, iy - yb->L, [&](int j) { return un[base + (long long)j * sy]; }, vdy, false, P.jv);
   } else {
     sy_ = (un[m - sy] * vdy[0] + un[m] * vdy[1]) + un[m + sy] * vdy[2];
   }
   if (zb) {
     const long long base = ix + (long long)P.nx * iy;
-    sz_ = mib_sum(*zb, zr, [&](int j) { return un[base + (long long)j * sz]; }, vdz, false, P.jv);
+    sz_ = mib_sum(*zb, iz - zb->L, [&](int j) { return un[base + (long long)j * sz]; }, vdz, false, P.jv);
   } else {
     sz_ = (un[m - sz] * vdz[0] + un[m] * vdz[1]) + un[m + sz] * vdz[2];
   }
   double src = source(P, E, side, ix, iy, iz);
-  if (xb) src = src_jumps(P, E, src, *xb, xr, vdx);
-  if (yb) src = src_jumps(P, E, src, *yb, yr, vdy);
-  if (zb) src = src_jumps(P, E, src, *zb, zr, vdz);
+  if (xb) src = src_jumps(P, E, src, *xb, ix - xb->L, vdx);
+  if (yb) src = src_jumps(P, E, src, *yb, iy - yb->L, vdy);
+  if (zb) src = src_jumps(P, E, src, *zb, iz - zb->L, vdz);
   return P.dt * (((sx + sy_) + sz_) + src);
 }
 
 // The Convert2Tri row operations of a line's blocks on its right-hand side
-// in shared memory (buf: the line's rows, stride 1), one lane per block.
+// in shared memory (buf: the line's rows, stride 1), and their rows' own q
+// into qbuf; one lane per block.
 template <int D>
-__device__ __forceinline__ void block_rows(const Dev& P, double* buf, int bfirst, int bend, int lane) {
+__device__ __forceinline__ void block_rows(const Dev& P, double* buf, double* qbuf, int bfirst, int bend, int lane,
+                                           bool ops) {
   for (int k = bfirst + lane; k < bend; k += 32) {
     const MibBlock& b = P.blk[D][k];
-    double* r = buf + b.L;
-    if (b.kind == 2) {
-      double r0 = r[0], r1 = r[1];
-      r1 -= b.rate[0] * r0;
-      r0 -= b.rate[1] * r1;
-      r[0] = r0;
-      r[1] = r1;
-    } else {
-      double r0 = r[0], r1 = r[1], r2 = r[2];
-      r1 -= b.rate[0] * r0;
-      r2 -= b.rate[1] * r0;
-      r0 -= b.rate[2] * r2;
-      r1 -= b.rate[3] * r2;
-      r2 -= b.rate[4] * r1;
-      r0 -= b.rate[5] * r1;
-      r[0] = r0;
-      r[1] = r1;
-      r[2] = r2;
+    const int L = b.L, kind = b.kind;
+    const double* const bq = P.fbq[D] + 3 * (long long)k;
+    double* r = buf + L;
+    if (ops) {
+      if (kind == 2) {
+        double r0 = r[0], r1 = r[1];
+        r1 -= b.rate[0] * r0;
+        r0 -= b.rate[1] * r1;
+        r[0] = r0;
+        r[1] = r1;
+      } else {
+        double r0 = r[0], r1 = r[1], r2 = r[2];
+        r1 -= b.rate[0] * r0;
+        r2 -= b.rate[1] * r0;
+        r0 -= b.rate[2] * r2;
+        r1 -= b.rate[3] * r2;
+        r2 -= b.rate[4] * r1;
+        r0 -= b.rate[5] * r1;
+        r[0] = r0;
+        r[1] = r1;
+        r[2] = r2;
+      }
     }
+    for (int q = 0; q < kind; q++) qbuf[L + q] = bq[q];
   }
 }
 
@@ -190,7 +206,7 @@ __device__ __forceinline__ double carry_down(double A, double B, int lane) {
 }
 
 // The segmented solve proper; IB(k), PP(k), QQ(k) give ib, p, q of the
-// lane's row jb + k (zero past the line end).
+// lane's row jb + k.
 template <int MX, class FI, class FP, class FQ>
 __device__ __forceinline__ void solve_seg(double* buf, int n, int lane, FI IB, FP PP, FQ QQ) {
   const int jb = lane * MX;
@@ -235,23 +251,23 @@ __device__ __forceinline__ void solve_seg(double* buf, int n, int lane, FI IB, F
   }
 }
 
-// A line without crossings: (ib, p, q) from the row table of its side in
-// shared memory, tab[0..R) = ib, tab[R..2R) = p, tab[2R..3R) = q.
+// A line without crossings: (ib, p) from the row table of its side in shared
+// memory, tab[0..R) = ib, tab[R..2R) = p, and q = p.
 template <int MX>
 __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n, int lane) {
   constexpr int R = 32 * MX;
   const int jb = lane * MX;
   solve_seg<MX>(
       buf, n, lane, [&](int k) { return tab[jb + k]; }, [&](int k) { return tab[R + jb + k]; },
-      [&](int k) { return tab[2 * R + jb + k]; });
+      [&](int k) { return tab[R + jb + k]; });
 }
 
 // A line that crosses the interface: the lane's rows of its own coefficients
-// (cf: [ib, p, q][R] in global memory, zero past the line end), loaded into
-// registers at once.
+// (cf: [ib, p][R] in global memory, zero past the line end), loaded into
+// registers at once; q from qbuf (p, with the block rows' own q over it).
 template <int MX>
 struct LineCoef {
-  double ib[MX], p[MX], q[MX];
+  double ib[MX], p[MX];
   __device__ __forceinline__ void load(const double* __restrict__ cf, int lane) {
     constexpr int R = 32 * MX;
     const int jb = lane * MX;
@@ -259,33 +275,26 @@ struct LineCoef {
     for (int k = 0; k < MX; k++) {
       ib[k] = __ldg(cf + jb + k);
       p[k] = __ldg(cf + R + jb + k);
-      q[k] = __ldg(cf + 2 * R + jb + k);
     }
+  }
+  // p as the q of the lane's rows, before the block rows' own go over it
+  __device__ __forceinline__ void put_q(double* qbuf, int lane) const {
+    const int jb = lane * MX;
+#pragma unroll
+    for (int k = 0; k < MX; k++) qbuf[jb + k] = p[k];
   }
 };
 template <int MX>
-__device__ __forceinline__ void solve_coef(double* buf, const LineCoef<MX>& c, int n, int lane) {
+__device__ __forceinline__ void solve_cross(double* buf, const double* qbuf, const LineCoef<MX>& c, int n, int lane) {
+  const int jb = lane * MX;
   solve_seg<MX>(
-      buf, n, lane, [&](int k) { return c.ib[k]; }, [&](int k) { return c.p[k]; }, [&](int k) { return c.q[k]; });
+      buf, n, lane, [&](int k) { return c.ib[k]; }, [&](int k) { return c.p[k]; },
+      [&](int k) { return qbuf[jb + k]; });
 }
 
-// What a line's solve needs to know about it, loaded ahead of its data.
-struct LineMeta {
-  int bfirst, bend, side1, cidx;
-};
-template <int D>
-__device__ __forceinline__ LineMeta line_meta(const Dev& P, long long lid) {
-  LineMeta m;
-  m.bfirst = P.bstart[D][lid];
-  m.bend = P.bstart[D][lid + 1];
-  m.side1 = (P.lside[D][lid] >> 1) & 1;
-  m.cidx = P.fcidx[D] ? P.fcidx[D][lid] : -1;
-  return m;
-}
-
-// Row tables [side][ib, p, q][R] into shared memory.
+// Row tables [side][ib, p][R] into shared memory.
 __device__ __forceinline__ void load_tab(double* s, const double* g, int R) {
-  for (int i = threadIdx.x; i < 6 * R; i += blockDim.x) s[i] = g[i];
+  for (int i = threadIdx.x; i < 4 * R; i += blockDim.x) s[i] = g[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -304,7 +313,7 @@ __global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, con
     double r[3] = {0.0, 0.0, 0.0};
     for (int q = 0; q < b.kind; q++) {
       const long long m = m0 + b.L + q;
-      r[q] = rho_mib(P, un, E, m, b.L + q, iy, iz, P.tag[m]);
+      r[q] = rho_mib(P, un, E, m, b.L + q, iy, iz, P.tag[m], P.mibref[P.xbmib[3 * t + q]]);
     }
     if (b.kind == 2) {
       r[1] -= b.rate[0] * r[0];
@@ -322,28 +331,92 @@ __global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, con
   }
   const long long k = t - nxb;
   if (k >= P.nmibnode) return;
+  const int4 ref = P.mibref[k];
+  if (ref.x >= 0) return;  // its x block's thread writes it
   const long long m = P.mibnode[k];
-  const int tg = P.tag[m];
-  if (tg & TAG_MIBX) return;  // its x block's thread writes it
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
-  d[m] = rho_mib(P, un, E, m, ix, iy, iz, tg);
+  d[m] = rho_mib(P, un, E, m, ix, iy, iz, P.tag[m], ref);
 }
 
 // ---------------------------------------------------------------------------
-// kf_x: rho fused with the x solves.
+// The x pass.
 
-constexpr int XW = 8;  // warps per CTA of kf_x: a 4 (y) x 2 (z) block of lines
+// Constants of rho along one x line.
+struct XLine {
+  double cx0, cy0, cz0, cx1, cy1, cz1;  // dt beta / h^2 of each direction, by side
+  double kin, koa, kob, yzE;           // source and boundary parts fixed along the line
+};
+__device__ __forceinline__ XLine x_line(const Dev& P, int iy, int iz, double E) {
+  XLine c;
+  c.cx0 = P.dt * P.vd[0][0][0];
+  c.cy0 = P.dt * P.vd[1][0][0];
+  c.cz0 = P.dt * P.vd[2][0][0];
+  c.cx1 = P.dt * P.vd[0][1][0];
+  c.cy1 = P.dt * P.vd[1][1][0];
+  c.cz1 = P.dt * P.vd[2][1][0];
+  const double yv = P.ax[1][iy], zv = P.ax[2][iz];
+  const double yz2 = yv * yv + zv * zv;
+  const bool eq8 = P.eq != 0;
+  // inside dt kin sin2x cos2y sin2z E; outside -dt E (x^2 + y^2 + z^2) -
+  // dt 6 beta_out E; on the faces (x^2 + y^2 + z^2) E
+  c.kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
+  c.koa = eq8 ? -P.dt * E : 0.0;
+  c.kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
+  c.yzE = yz2 * E;
+  return c;
+}
 
+// rho of interior x line (iy, iz) into buf[j] (j = lane + 32 k, coalesced
+// loads); MIB rows take kf_mib's value from d.
 template <int MX>
-__host__ __device__ constexpr size_t x_smem() {
-  // row tables 6 R, one line buffer of R doubles per warp
-  return sizeof(double) * ((size_t)6 * 32 * MX + (size_t)XW * 32 * MX);
+__device__ __forceinline__ void x_rho(const Dev& P, const double* __restrict__ un, const double* __restrict__ d,
+                                      double E, int iy, int iz, double* buf, int lane) {
+  const int nx = P.nx;
+  const long long sy = nx, sz = (long long)nx * P.ny;
+  const long long m0 = (long long)nx * (iy + (long long)P.ny * iz);
+  const XLine c = x_line(P, iy, iz, E);
+  const bool eq8 = P.eq != 0;
+  const double* const ur = un + m0;
+  const unsigned char* const tr = P.tag + m0;
+#pragma unroll 3
+  for (int k = 0; k < MX; k++) {
+    const int j = lane + 32 * k;
+    if (j < nx) {
+      // (an interior line: every neighbour index lies inside the field)
+      const int t = tr[j];
+      const double uc = ur[j], uxm = ur[j - 1], uxp = ur[j + 1];
+      const double uym = ur[j - sy], uyp = ur[j + sy], uzm = ur[j - sz], uzp = ur[j + sz];
+      const double x = P.ax[0][j], s2x = P.s2[0][j];
+      double r;
+      if (j == 0 || j == nx - 1) {
+        r = (eq8 ? fma(x * x, E, c.yzE) : 100.0) - uc;
+      } else if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
+        r = d[m0 + j];  // from kf_mib
+      } else {
+        const double lx = fma(-2.0, uc, uxm + uxp);
+        const double ly = fma(-2.0, uc, uym + uyp);
+        const double lz = fma(-2.0, uc, uzm + uzp);
+        if (t & TAG_OUT)
+          r = fma(c.cx1, lx, fma(c.cy1, ly, fma(c.cz1, lz, fma(c.koa, x * x, c.kob))));
+        else
+          r = fma(c.cx0, lx, fma(c.cy0, ly, fma(c.cz0, lz, c.kin * s2x)));
+      }
+      buf[j] = r;
+    }
+  }
 }
 
 template <int MX>
-__global__ void __launch_bounds__(32 * XW, 3) kf_x(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                   double* __restrict__ dst, double E) {
+__host__ __device__ constexpr size_t xr_smem() {
+  // row tables 4 R, one line buffer of R doubles per warp
+  return sizeof(double) * ((size_t)4 * 32 * MX + (size_t)XW * 32 * MX);
+}
+
+// The regular x lines and the face lines.
+template <int MX>
+__global__ void __launch_bounds__(32 * XW, 4) kf_xr(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                    double* __restrict__ dst, double E) {
   constexpr int R = 32 * MX;
   extern __shared__ __align__(16) double smx[];
   double* const stab = smx;
@@ -352,107 +425,123 @@ __global__ void __launch_bounds__(32 * XW, 3) kf_x(const __grid_constant__ Dev P
   E = step_e(P, E, 2);
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* const buf = smx + 6 * R + w * R;
+  double* const buf = smx + 4 * R + w * R;
   const bool eq8 = P.eq != 0;
-  const long long sy = nx, sz = (long long)nx * ny;
-  // dt beta / h^2 of each direction, by side
-  const double cx0 = P.dt * P.vd[0][0][0], cy0 = P.dt * P.vd[1][0][0], cz0 = P.dt * P.vd[2][0][0];
-  const double cx1 = P.dt * P.vd[0][1][0], cy1 = P.dt * P.vd[1][1][0], cz1 = P.dt * P.vd[2][1][0];
   const int nbY = (ny + 3) / 4, nbZ = (nz + 1) / 2;
   const long long nb = (long long)nbY * nbZ;
+  auto line_of = [&](long long blk, int& iy, int& iz) {
+    iy = (int)(blk % nbY) * 4 + (w & 3);
+    iz = (int)(blk / nbY) * 2 + (w >> 2);
+  };
+  auto flags_of = [&](long long blk) -> int {
+    if (blk >= nb) return 0;
+    int iy, iz;
+    line_of(blk, iy, iz);
+    if (iy >= ny || iz >= nz) return 0;
+    return P.fline[0][(long long)iy * nz + iz];
+  };
+  // the line flags (crossing, side of row 1) are read one line ahead
+  int fl = flags_of(blockIdx.x);
   for (long long blk = blockIdx.x; blk < nb; blk += gridDim.x) {
-    const int iy = (int)(blk % nbY) * 4 + (w & 3), iz = (int)(blk / nbY) * 2 + (w >> 2);
+    const int f = fl;
+    fl = flags_of(blk + gridDim.x);
+    int iy, iz;
+    line_of(blk, iy, iz);
     if (iy >= ny || iz >= nz) continue;  // (warp-uniform)
     const long long m0 = (long long)nx * (iy + (long long)ny * iz);
-    const double yv = P.ax[1][iy], zv = P.ax[2][iz];
-    const double yz2 = yv * yv + zv * zv;
     if (iy == 0 || iz == 0 || iy == ny - 1 || iz == nz - 1) {
       // face line: d = Outer_u(t_next) - u^n
+      const double yv = P.ax[1][iy], zv = P.ax[2][iz];
+      const double yz2 = yv * yv + zv * zv;
       for (int j = lane; j < nx; j += 32) {
         const double x = P.ax[0][j];
         dst[m0 + j] = (eq8 ? (x * x + yz2) * E : 100.0) - un[m0 + j];
       }
       continue;
     }
-    const long long lid = (long long)iy * nz + iz;
-    const LineMeta lm = line_meta<0>(P, lid);
-    // source constants of the line: inside dt kin sin2x cos2y sin2z E,
-    // outside -dt E (x^2 + y^2 + z^2) - dt 6 beta_out E
-    const double kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
-    const double koa = eq8 ? -P.dt * E : 0.0;
-    const double kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
-    const double* const ur = un + m0;
-    const unsigned char* const tr = P.tag + m0;
-#pragma unroll 3
-    for (int k = 0; k < MX; k++) {
-      const int j = lane + 32 * k;
-      if (j < nx) {
-        // (an interior line: every neighbour index lies inside the field)
-        const int t = tr[j];
-        const double uc = ur[j], uxm = ur[j - 1], uxp = ur[j + 1];
-        const double uym = ur[j - sy], uyp = ur[j + sy], uzm = ur[j - sz], uzp = ur[j + sz];
-        const double x = P.ax[0][j], s2x = P.s2[0][j];
-        double r;
-        if (j == 0 || j == nx - 1) {
-          r = (eq8 ? fma(x * x, E, yz2 * E) : 100.0) - uc;
-        } else if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
-          r = dst[m0 + j];  // from kf_mib
-        } else {
-          const double lx = fma(-2.0, uc, uxm + uxp);
-          const double ly = fma(-2.0, uc, uym + uyp);
-          const double lz = fma(-2.0, uc, uzm + uzp);
-          if (t & TAG_OUT)
-            r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, x * x, kob))));
-          else
-            r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * s2x)));
-        }
-        buf[j] = r;
-      }
-    }
+    if (f & 1) continue;  // crosses the interface: kf_xc
+    x_rho<MX>(P, un, dst, E, iy, iz, buf, lane);
     __syncwarp();
-    if (lm.bend > lm.bfirst) {
-      LineCoef<MX> c;
-      c.load(P.fcoef[0] + (size_t)lm.cidx * 3 * R, lane);
-      solve_coef<MX>(buf, c, nx, lane);
-    } else {
-      solve_tab<MX>(buf, stab + lm.side1 * 3 * R, nx, lane);
-    }
+    solve_tab<MX>(buf, stab + ((f >> 1) & 1) * 2 * R, nx, lane);
     __syncwarp();
     for (int j = lane; j < nx; j += 32) dst[m0 + j] = buf[j];
     __syncwarp();  // the buffer is free for the next line
   }
 }
 
-// ---------------------------------------------------------------------------
-// kf_yz: y solves in place on d*, z solves with the accumulation into u.
-
 template <int MX>
-__host__ __device__ constexpr size_t yz_smem() {
-  // row tables 6 R, two buffers of NL lines x (R + 1) doubles
-  return sizeof(double) * ((size_t)6 * 32 * MX + (size_t)2 * YZ_NL * (32 * MX + 1));
+__host__ __device__ constexpr size_t cross_smem() {
+  // per warp a line buffer and its q
+  return sizeof(double) * (size_t)CW * 2 * 32 * MX;
 }
 
+// The x lines that cross the interface, one warp per line.
+template <int MX>
+__global__ void __launch_bounds__(32 * CW, 3) kf_xc(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                    double* __restrict__ dst, double E) {
+  constexpr int R = 32 * MX;
+  extern __shared__ __align__(16) double smc[];
+  E = step_e(P, E, 2);
+  const int nx = P.nx, nz = P.nz;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* const buf = smc + 2 * w * R;
+  double* const qbuf = buf + R;
+  const int nc = P.nfcross[0];
+  for (int c = blockIdx.x * CW + w; c < nc; c += gridDim.x * CW) {
+    const long long lid = P.fcross[0][c];
+    const int iy = (int)(lid / nz), iz = (int)(lid % nz);
+    const int bfirst = P.bstart[0][lid], bend = P.bstart[0][lid + 1];
+    LineCoef<MX> cf;
+    cf.load(P.fcoef[0] + (size_t)c * 2 * R, lane);
+    x_rho<MX>(P, un, dst, E, iy, iz, buf, lane);
+    cf.put_q(qbuf, lane);
+    __syncwarp();
+    block_rows<0>(P, buf, qbuf, bfirst, bend, lane, false);  // (the row operations were done by kf_mib)
+    __syncwarp();
+    solve_cross<MX>(buf, qbuf, cf, nx, lane);
+    __syncwarp();
+    const long long m0 = (long long)nx * (iy + (long long)P.ny * iz);
+    for (int j = lane; j < nx; j += 32) dst[m0 + j] = buf[j];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The y and z passes.
+
+template <int MX, bool ACC>
+__host__ __device__ constexpr size_t yt_smem() {
+  // row tables 4 R; two buffers of NL lines x (R + 1) doubles; ACC: one
+  // buffer of u^n
+  return sizeof(double) * ((size_t)4 * 32 * MX + (size_t)(ACC ? 3 : 2) * YZ_NL * (32 * MX + 1));
+}
+
+// The regular lines of direction D in tiles: y in place on d*; z (ACC) with
+// the update of u, face lines included (their d** passes through).
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * YZ_NL, 3) kf_yz(const __grid_constant__ Dev P, double* __restrict__ f,
-                                                        double* __restrict__ u, int ntiles) {
+__global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_constant__ Dev P,
+                                                                  double* __restrict__ f, double* __restrict__ u,
+                                                                  int ntiles) {
   static_assert(D == 1 || D == 2, "y and z lines");
   constexpr int R = 32 * MX;
   constexpr int LS = R + 1;  // odd: a copy's lines and a lane's stride-MX rows fall on distinct banks
   extern __shared__ __align__(16) double smyz[];
   double* const stab = smyz;
-  double* const bufs = smyz + 6 * R;
+  double* const bufs = smyz + 4 * R;
+  double* const ubuf = bufs + 2 * YZ_NL * LS;  // (ACC)
   const int nx = P.nx;
   const int n = D == 1 ? P.ny : P.nz;
   const int n2 = D == 1 ? P.nz : P.ny;  // the second line index: iz (y lines) or iy (z lines)
   const long long s = D == 1 ? (long long)nx : (long long)nx * P.ny;   // row stride
   const long long s2 = D == 1 ? (long long)nx * P.ny : (long long)nx;  // stride of the second line index
   // y tiles cover the interior lines (face y lines keep d*); z tiles cover
-  // every line (face z lines pass d** through to the accumulation)
+  // every line (face z lines pass d** through to the update)
   const int i1lo = ACC ? 0 : 1, i1n = ACC ? nx : nx - 2;
   const int i2lo = ACC ? 0 : 1;
   const int tpr = (i1n + YZ_NL - 1) / YZ_NL;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int c = threadIdx.x % YZ_NL, jc = threadIdx.x / YZ_NL;  // this thread's copy share: line c, rows jc + 32 m
+  const uint8_t* const fline = P.fline[D];
 
   load_tab(stab, P.ftab[D], R);
 
@@ -467,16 +556,21 @@ __global__ void __launch_bounds__(32 * YZ_NL, 3) kf_yz(const __grid_constant__ D
     T.ok = t < ntiles;
     return T;
   };
-  // line c of tile T: its first element
-  auto copy_in = [&](const Tile& T, double* buf) {
-    const int i1 = T.i1 + c;
-    if (T.ok && i1 < i1lo + i1n) {
-      const long long g0 = i1 + s2 * T.i2 + (long long)jc * s;
+  // flags of line i of tile T (-1: no line there); bit0 crosses the
+  // interface (left to kf_yc), bit1 side of row 1
+  auto flags = [&](const Tile& T, int i) -> int {
+    const int i1 = T.i1 + i;
+    if (!T.ok || i1 >= i1lo + i1n) return -1;
+    return fline[(long long)i1 * n2 + T.i2];
+  };
+  auto copy_rows = [&](const Tile& T, int fc, const double* src, double* buf) {
+    if (fc >= 0 && !(fc & 1)) {
+      const long long g0 = T.i1 + c + s2 * T.i2 + (long long)jc * s;
       double* const cb = buf + c * LS;
 #pragma unroll
       for (int m = 0; m < MX; m++) {
         const int j = jc + 32 * m;
-        if (j < n) cp_async8(cb + j, f + g0 + (long long)32 * m * s);
+        if (j < n) cp_async8(cb + j, src + g0 + (long long)32 * m * s);
       }
     }
     cp_async_commit();
@@ -484,63 +578,112 @@ __global__ void __launch_bounds__(32 * YZ_NL, 3) kf_yz(const __grid_constant__ D
 
   int t = blockIdx.x;
   Tile cur = tile_of(t);
-  copy_in(cur, bufs);
+  Tile nxt = tile_of(t + gridDim.x);
+  // flags are read two tiles ahead: this thread's copy line (fc*) and this
+  // warp's solve line (fw*)
+  int fc0 = flags(cur, c), fc1 = flags(nxt, c);
+  int fw0 = flags(cur, w), fw1 = flags(nxt, w);
+  copy_rows(cur, fc0, f, bufs);
   for (int it = 0; cur.ok; it++) {
-    const Tile nxt = tile_of(t + gridDim.x);
+    const Tile nx2 = tile_of(t + 2 * gridDim.x);
+    const int fc2 = flags(nx2, c), fw2 = flags(nx2, w);
     double* const buf = bufs + (size_t)(it & 1) * YZ_NL * LS;
-    copy_in(nxt, bufs + (size_t)((it + 1) & 1) * YZ_NL * LS);
-    // warp w's line of this tile: what its solve needs, loaded before the
-    // tile's data has landed
-    const int i1w = cur.i1 + w;
-    const bool solve = i1w < i1lo + i1n && i1w >= 1 && i1w <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
-    LineMeta lm{0, 0, 0, -1};
-    const long long lid = (long long)i1w * n2 + cur.i2;
-    if (solve) lm = line_meta<D>(P, lid);
-    cp_async_wait<1>();
-    __syncthreads();
-    if (solve) {
-      double* const lb = buf + w * LS;
-      if (lm.bend > lm.bfirst) {
-        LineCoef<MX> cf;
-        cf.load(P.fcoef[D] + (size_t)lm.cidx * 3 * R, lane);
-        block_rows<D>(P, lb, lm.bfirst, lm.bend, lane);
-        __syncwarp();
-        solve_coef<MX>(lb, cf, n, lane);
-      } else {
-        solve_tab<MX>(lb, stab + lm.side1 * 3 * R, n, lane);
-      }
-    }
+    if (ACC) copy_rows(cur, fc0, u, ubuf);
+    copy_rows(nxt, fc1, f, bufs + (size_t)((it + 1) & 1) * YZ_NL * LS);
+    if (ACC)
+      cp_async_wait<2>();
+    else
+      cp_async_wait<1>();
     __syncthreads();
     {
-      const int i1 = cur.i1 + c;
-      if (i1 < i1lo + i1n) {
-        const long long g0 = i1 + s2 * cur.i2 + (long long)jc * s;
-        const double* const cb = buf + c * LS;
-        if (ACC) {
-          double uv[MX];
+      const int i1 = cur.i1 + w;
+      const bool interior = i1 >= 1 && i1 <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
+      if (fw0 >= 0 && !(fw0 & 1) && interior) solve_tab<MX>(buf + w * LS, stab + ((fw0 >> 1) & 1) * 2 * R, n, lane);
+    }
+    if (ACC) cp_async_wait<1>();
+    __syncthreads();
+    if (fc0 >= 0 && !(fc0 & 1)) {
+      const long long g0 = cur.i1 + c + s2 * cur.i2 + (long long)jc * s;
+      const double* const cb = buf + c * LS;
 #pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) uv[m] = u[g0 + (long long)32 * m * s];
-#pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) u[g0 + (long long)32 * m * s] = uv[m] + cb[jc + 32 * m];
-        } else {
-#pragma unroll
-          for (int m = 0; m < MX; m++)
-            if (jc + 32 * m < n) f[g0 + (long long)32 * m * s] = cb[jc + 32 * m];
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) {
+          if (ACC)
+            u[g0 + (long long)32 * m * s] = ubuf[c * LS + j] + cb[j];
+          else
+            f[g0 + (long long)32 * m * s] = cb[j];
         }
       }
     }
     t += gridDim.x;
     cur = nxt;
+    nxt = nx2;
+    fc0 = fc1;
+    fc1 = fc2;
+    fw0 = fw1;
+    fw1 = fw2;
   }
   cp_async_wait<0>();
+}
+
+// The lines of direction D that cross the interface, one warp per line:
+// y in place on d*, z (ACC) with the update of u.
+template <int D, int MX, bool ACC>
+__global__ void __launch_bounds__(32 * CW, 3) kf_yc(const __grid_constant__ Dev P, double* __restrict__ f,
+                                                    double* __restrict__ u) {
+  static_assert(D == 1 || D == 2, "y and z lines");
+  constexpr int R = 32 * MX;
+  extern __shared__ __align__(16) double smc[];
+  const int nx = P.nx;
+  const int n = D == 1 ? P.ny : P.nz;
+  const int n2 = D == 1 ? P.nz : P.ny;
+  const long long s = D == 1 ? (long long)nx : (long long)nx * P.ny;
+  const long long s2 = D == 1 ? (long long)nx * P.ny : (long long)nx;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* const buf = smc + 2 * w * R;
+  double* const qbuf = buf + R;
+  const int jb = lane * MX;
+  const int nc = P.nfcross[D];
+  for (int c = blockIdx.x * CW + w; c < nc; c += gridDim.x * CW) {
+    const long long lid = P.fcross[D][c];
+    const long long base = lid / n2 + s2 * (lid % n2);
+    const int bfirst = P.bstart[D][lid], bend = P.bstart[D][lid + 1];
+    LineCoef<MX> cf;
+    cf.load(P.fcoef[D] + (size_t)c * 2 * R, lane);
+    double uv[MX];
+#pragma unroll
+    for (int k = 0; k < MX; k++) {
+      const int j = jb + k;
+      if (j < n) {
+        buf[j] = f[base + (long long)j * s];
+        if (ACC) uv[k] = u[base + (long long)j * s];
+      }
+    }
+    cf.put_q(qbuf, lane);
+    __syncwarp();
+    block_rows<D>(P, buf, qbuf, bfirst, bend, lane, true);
+    __syncwarp();
+    solve_cross<MX>(buf, qbuf, cf, n, lane);
+    // (each lane reads back the rows it wrote)
+#pragma unroll
+    for (int k = 0; k < MX; k++) {
+      const int j = jb + k;
+      if (j < n) {
+        if (ACC)
+          u[base + (long long)j * s] = uv[k] + buf[j];
+        else
+          f[base + (long long)j * s] = buf[j];
+      }
+    }
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Set-up of the form (once per handle).
 
-// Row tables of direction D: [side][ib, p, q][R] from the prefix factors of
+// Row tables of direction D: [side][ib, p][R] from the prefix factors of
 // that side (ptab: bet_j, gam_j); zero past the line end.
 template <int D>
 __global__ void __launch_bounds__(TPB) kf_tab(const __grid_constant__ Dev P, double* tab, int R) {
@@ -548,45 +691,72 @@ __global__ void __launch_bounds__(TPB) kf_tab(const __grid_constant__ Dev P, dou
   const int i = blockIdx.x * TPB + threadIdx.x;
   if (i >= 2 * R) return;
   const int side = i / R, j = i % R;
-  double ib = 0.0, p = 0.0, q = 0.0;
+  double ib = 0.0, p = 0.0;
   if (j < n) {
-    const double* pt = P.ptab[D][side];
+    const double bet = P.ptab[D][side][2 * j];
     const double a = (j == 0 || j == n - 1) ? 0.0 : P.ia[D][side];
-    ib = 1.0 / pt[2 * j];
-    p = -a * ib;
-    q = j == n - 1 ? 0.0 : -pt[2 * (j + 1) + 1];
+    ib = 1.0 / bet;
+    p = -(a / bet);
   }
-  double* T = tab + (size_t)side * 3 * R;
+  double* T = tab + (size_t)side * 2 * R;
   T[j] = ib;
   T[R + j] = p;
-  T[2 * R + j] = q;
 }
 
-// Coefficients of the lines that cross the interface, one thread per line,
-// walking the line as the sequential sweep does (the factors from the prefix
-// table before the first MIB row and per node from it on; the regular rows'
-// side from the line's start and after each block), into the line's slot c
-// of cf: [c][ib, p, q][R].
+// Per line of direction D: bit0 the line crosses the interface (has MIB
+// blocks), bit1 the side of its row 1.  Face lines: 0.
 template <int D>
-__global__ void __launch_bounds__(TPB) kf_coef(const __grid_constant__ Dev P, double* cf, int R) {
+__global__ void __launch_bounds__(TPB) kf_fline(const __grid_constant__ Dev P, uint8_t* fl) {
   const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
   if (t >= nlines<D>(P)) return;
   Line L;
   decode_line<D>(P, t, L);
-  if (L.boundary) return;
-  const int bfirst = P.bstart[D][L.lid], bend = P.bstart[D][L.lid + 1];
-  if (bfirst == bend) return;
-  const int n = L.n;
-  const long long s = L.s;
+  uint8_t v = 0;
+  if (!L.boundary) {
+    v = (uint8_t)(((P.lside[D][L.lid] >> 1) & 1) << 1);
+    if (P.bstart[D][L.lid + 1] > P.bstart[D][L.lid]) v |= 1;
+  }
+  fl[L.lid] = v;
+}
+
+// Line geometry from a line id (i1 * n2 + i2) of direction D.
+template <int D>
+__device__ __forceinline__ void line_at(const Dev& P, long long lid, long long& base, long long& s) {
+  const int n2 = D == 2 ? P.ny : P.nz;
+  const int i1 = (int)(lid / n2), i2 = (int)(lid % n2);
+  if (D == 0) {
+    base = (long long)P.nx * (i1 + (long long)P.ny * i2);
+    s = 1;
+  } else if (D == 1) {
+    base = i1 + (long long)P.nx * P.ny * i2;
+    s = P.nx;
+  } else {
+    base = i1 + (long long)P.nx * i2;
+    s = (long long)P.nx * P.ny;
+  }
+}
+
+// Coefficients (ib, p) of the crossing lines, one thread per listed line,
+// walking the line as the sequential sweep does (the factors from the
+// prefix table before the first MIB row and per node from it on; the regular
+// rows' side from the line's start and after each block), into cf[c][2][R].
+template <int D>
+__global__ void __launch_bounds__(TPB) kf_coef(const __grid_constant__ Dev P, double* cf, int R) {
+  const int c = blockIdx.x * TPB + threadIdx.x;
+  if (c >= P.nfcross[D]) return;
+  const long long lid = P.fcross[D][c];
+  const int n = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
+  long long base, s;
+  line_at<D>(P, lid, base, s);
+  const int bfirst = P.bstart[D][lid], bend = P.bstart[D][lid + 1];
   const MibBlock* const blk = P.blk[D];
   const int L1 = blk[bfirst].L;
-  const int side1 = (P.lside[D][L.lid] >> 1) & 1;
+  const int side1 = (P.lside[D][lid] >> 1) & 1;
   const double* const pt = P.ptab[D][side1];
-  double* const c = cf + (size_t)P.fcidx[D][L.lid] * 3 * R;
+  double* const o = cf + (size_t)c * 2 * R;
   int b = bfirst, side = side1;
   for (int j = 0; j < n; j++) {
-    const long long g = L.base + (long long)j * s;
-    const double bet = j >= L1 ? P.fbet[D][g] : pt[2 * j];
+    const double bet = j >= L1 ? P.fbet[D][base + (long long)j * s] : pt[2 * j];
     double a;
     if (j == 0 || j == n - 1) {
       a = 0.0;
@@ -600,15 +770,55 @@ __global__ void __launch_bounds__(TPB) kf_coef(const __grid_constant__ Dev P, do
     } else {
       a = P.ia[D][side];
     }
-    const double gn = j == n - 1 ? 0.0 : j + 1 >= L1 ? P.fgam[D][g + s] : pt[2 * (j + 1) + 1];
-    c[j] = 1.0 / bet;
-    c[R + j] = -(a / bet);
-    c[2 * R + j] = -gn;
+    o[j] = 1.0 / bet;
+    o[R + j] = -(a / bet);
   }
 }
 
+// q = -gam_{j+1} of the rows of each block of direction D (their c is not
+// their a), from the per-node factors: bq[3 k + r].
+template <int D>
+__global__ void __launch_bounds__(TPB) kf_bq(const __grid_constant__ Dev P, double* bq) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= P.nblk[D]) return;
+  const MibBlock& b = P.blk[D][k];
+  long long base, s;
+  line_at<D>(P, b.line, base, s);
+  for (int r = 0; r < 3; r++)
+    bq[3 * (long long)k + r] = r < b.kind ? -P.fgam[D][base + (long long)(b.L + r + 1) * s] : 0.0;
+}
+
+// Per MIB node: its block in each direction (-1: none); for the x blocks,
+// the MIB node index of each of their rows.
+__global__ void __launch_bounds__(TPB) kf_mibref(const __grid_constant__ Dev P, int4* ref, int32_t* xbmib) {
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k >= P.nmibnode) return;
+  const long long m = P.mibnode[k];
+  const int tg = P.tag[m];
+  int ix, iy, iz;
+  node_xyz(P, m, ix, iy, iz);
+  int4 r = make_int4(-1, -1, -1, 0);
+  int row = 0;
+  if (tg & TAG_MIBX) {
+    const MibBlock* b = find_block<0>(P, iy * P.nz + iz, ix, row);
+    if (b) {
+      r.x = (int)(b - P.blk[0]);
+      xbmib[3 * r.x + row] = k;
+    }
+  }
+  if (tg & TAG_MIBY) {
+    const MibBlock* b = find_block<1>(P, ix * P.nz + iz, iy, row);
+    if (b) r.y = (int)(b - P.blk[1]);
+  }
+  if (tg & TAG_MIBZ) {
+    const MibBlock* b = find_block<2>(P, ix * P.ny + iy, iz, row);
+    if (b) r.z = (int)(b - P.blk[2]);
+  }
+  ref[k] = r;
+}
+
 // ---------------------------------------------------------------------------
-// Launch shapes
+// Launches
 
 int fast_mx(int n) {
   const int c[6] = {1, 3, 5, 9, 13, 17};
@@ -617,49 +827,56 @@ int fast_mx(int n) {
   return 0;
 }
 
-template <int MX>
-void launch_x(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
+template <class K>
+int resident_grid(const Dev& P, K kernel, int threads, size_t smem, long long want) {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_x<MX>, 32 * XW, x_smem<MX>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   if (per_sm < 1) per_sm = 1;
-  const long long nb = (long long)((P.ny + 3) / 4) * ((P.nz + 1) / 2);
-  const int grid = (int)std::max(1LL, std::min(nb, (long long)per_sm * P.sweep_blocks));
-  kf_x<MX><<<grid, 32 * XW, x_smem<MX>(), st>>>(P, un, d, E);
+  return (int)std::max(1LL, std::min(want, (long long)per_sm * P.sweep_blocks));
 }
 
+template <int MX>
+void launch_xr(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
+  const long long nb = (long long)((P.ny + 3) / 4) * ((P.nz + 1) / 2);
+  const int grid = resident_grid(P, kf_xr<MX>, 32 * XW, xr_smem<MX>(), nb);
+  kf_xr<MX><<<grid, 32 * XW, xr_smem<MX>(), st>>>(P, un, d, E);
+}
+template <int MX>
+void launch_xc(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
+  const int grid = resident_grid(P, kf_xc<MX>, 32 * CW, cross_smem<MX>(), (P.nfcross[0] + CW - 1) / CW);
+  kf_xc<MX><<<grid, 32 * CW, cross_smem<MX>(), st>>>(P, un, d, E);
+}
 template <int D, int MX, bool ACC>
-void launch_yz(const Dev& P, double* f, double* u, cudaStream_t st) {
+void launch_yt(const Dev& P, double* f, double* u, cudaStream_t st) {
   const int i1n = ACC ? P.nx : P.nx - 2;
   const int n2 = D == 1 ? P.nz : P.ny;
   const int rows = ACC ? n2 : n2 - 2;
   const int ntiles = (i1n + YZ_NL - 1) / YZ_NL * rows;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_yz<D, MX, ACC>, 32 * YZ_NL, yz_smem<MX>());
-  if (per_sm < 1) per_sm = 1;
-  const int grid = std::max(1, std::min(ntiles, per_sm * P.sweep_blocks));
-  kf_yz<D, MX, ACC><<<grid, 32 * YZ_NL, yz_smem<MX>(), st>>>(P, f, u, ntiles);
+  const int grid = resident_grid(P, kf_yt<D, MX, ACC>, 32 * YZ_NL, yt_smem<MX, ACC>(), ntiles);
+  kf_yt<D, MX, ACC><<<grid, 32 * YZ_NL, yt_smem<MX, ACC>(), st>>>(P, f, u, ntiles);
+}
+template <int D, int MX, bool ACC>
+void launch_yc(const Dev& P, double* f, double* u, cudaStream_t st) {
+  const int grid = resident_grid(P, kf_yc<D, MX, ACC>, 32 * CW, cross_smem<MX>(), (P.nfcross[D] + CW - 1) / CW);
+  kf_yc<D, MX, ACC><<<grid, 32 * CW, cross_smem<MX>(), st>>>(P, f, u);
 }
 
 #define MTS_FAST_MX(X) X(1) X(3) X(5) X(9) X(13) X(17)
 
-template <int D, bool ACC>
-void launch_yz_n(const Dev& P, double* f, double* u, cudaStream_t st) {
-  const int n = D == 1 ? P.ny : P.nz;
+// The regular (crossing = false) or crossing lines' launch of direction d,
+// dispatched on its rows per lane.
+void launch_dir(const Dev& P, int d, bool crossing, const double* un, double* f, double* u, double E,
+                cudaStream_t st) {
+  const int n = d == 0 ? P.nx : d == 1 ? P.ny : P.nz;
   switch (fast_mx(n)) {
-#define MTS_CASE(mx) \
-  case mx:           \
-    launch_yz<D, mx, ACC>(P, f, u, st); \
-    break;
-    MTS_FAST_MX(MTS_CASE)
-#undef MTS_CASE
-  }
-}
-
-void launch_x_n(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  switch (fast_mx(P.nx)) {
-#define MTS_CASE(mx) \
-  case mx:           \
-    launch_x<mx>(P, un, d, E, st); \
+#define MTS_CASE(mx)                                                     \
+  case mx:                                                               \
+    if (d == 0 && !crossing) launch_xr<mx>(P, un, f, E, st);             \
+    if (d == 0 && crossing) launch_xc<mx>(P, un, f, E, st);              \
+    if (d == 1 && !crossing) launch_yt<1, mx, false>(P, f, nullptr, st); \
+    if (d == 1 && crossing) launch_yc<1, mx, false>(P, f, nullptr, st);  \
+    if (d == 2 && !crossing) launch_yt<2, mx, true>(P, f, u, st);        \
+    if (d == 2 && crossing) launch_yc<2, mx, true>(P, f, u, st);         \
     break;
     MTS_FAST_MX(MTS_CASE)
 #undef MTS_CASE
@@ -668,9 +885,13 @@ void launch_x_n(const Dev& P, const double* un, double* d, double E, cudaStream_
 
 template <int MX>
 void fast_attr() {
-  cudaFuncSetAttribute(kf_x<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x_smem<MX>());
-  cudaFuncSetAttribute(kf_yz<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yz_smem<MX>());
-  cudaFuncSetAttribute(kf_yz<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yz_smem<MX>());
+  cudaFuncSetAttribute(kf_xr<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem<MX>());
+  cudaFuncSetAttribute(kf_xc<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
+  cudaFuncSetAttribute(kf_yt<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yt_smem<MX, false>());
+  cudaFuncSetAttribute(kf_yt<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yt_smem<MX, true>());
+  cudaFuncSetAttribute(kf_yc<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
+  cudaFuncSetAttribute(kf_yc<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
 }
 
 }  // namespace
@@ -683,9 +904,13 @@ void configure_fast_kernels() {
 
 int fast_rows_per_lane(int n) { return fast_mx(n); }
 
-bool fast_fits(int nx, int ny, int nz) {
-  const int mx = fast_mx(nx), my = fast_mx(ny), mz = fast_mx(nz);
-  return mx && my && mz;
+bool fast_fits(int nx, int ny, int nz) { return fast_mx(nx) && fast_mx(ny) && fast_mx(nz); }
+
+int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t st) {
+  kf_fline<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, fline[0]);
+  kf_fline<1><<<(unsigned)((nlines<1>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, fline[1]);
+  kf_fline<2><<<(unsigned)((nlines<2>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, fline[2]);
+  return 3;
 }
 
 int build_fast_tables(const Dev& P, cudaStream_t st) {
@@ -701,32 +926,68 @@ int build_fast_tables(const Dev& P, cudaStream_t st) {
     launches++;
     if (P.nblk[d] == 0) continue;
     double* cf = const_cast<double*>(P.fcoef[d]);
-    if (d == 0) kf_coef<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
-    if (d == 1) kf_coef<1><<<(unsigned)((nlines<1>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
-    if (d == 2) kf_coef<2><<<(unsigned)((nlines<2>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, cf, R);
+    double* bq = const_cast<double*>(P.fbq[d]);
+    const unsigned gc = (unsigned)((P.nfcross[d] + TPB - 1) / TPB);
+    const unsigned gb = (unsigned)((P.nblk[d] + TPB - 1) / TPB);
+    if (d == 0) {
+      if (gc) kf_coef<0><<<gc, TPB, 0, st>>>(P, cf, R);
+      kf_bq<0><<<gb, TPB, 0, st>>>(P, bq);
+    }
+    if (d == 1) {
+      if (gc) kf_coef<1><<<gc, TPB, 0, st>>>(P, cf, R);
+      kf_bq<1><<<gb, TPB, 0, st>>>(P, bq);
+    }
+    if (d == 2) {
+      if (gc) kf_coef<2><<<gc, TPB, 0, st>>>(P, cf, R);
+      kf_bq<2><<<gb, TPB, 0, st>>>(P, bq);
+    }
+    launches += 2;
+  }
+  if (P.nmibnode > 0) {
+    kf_mibref<<<(unsigned)((P.nmibnode + TPB - 1) / TPB), TPB, 0, st>>>(P, const_cast<int4*>(P.mibref),
+                                                                        const_cast<int32_t*>(P.xbmib));
     launches++;
   }
   return launches;
 }
 
-int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cudaStream_t st, cudaEvent_t* ev) {
+int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cudaStream_t st, cudaEvent_t* ev,
+                     const SideStream* side) {
+  int launches = 0;
   auto mark = [&](int k) {
     if (ev) cudaEventRecord(ev[k], st);
   };
-  int launches = 3;
+  // The crossing lines' kernels run on the side stream beside the regular
+  // lines' (the two write disjoint lines).
+  const bool two = side && side->stream;
+  auto pass = [&](int dir, const double* un, double* f, double* uu, double E) {
+    const bool cross = P.nfcross[dir] > 0;
+    if (cross && two) {
+      cudaEventRecord(side->fork, st);
+      cudaStreamWaitEvent(side->stream, side->fork, 0);
+      launch_dir(P, dir, true, un, f, uu, E, side->stream);
+    }
+    launch_dir(P, dir, false, un, f, uu, E, st);
+    if (cross && !two) launch_dir(P, dir, true, un, f, uu, E, st);
+    if (cross && two) {
+      cudaEventRecord(side->join, side->stream);
+      cudaStreamWaitEvent(st, side->join, 0);
+    }
+    launches += cross ? 2 : 1;
+  };
   mark(0);
   if (P.nblk[0] > 0 || P.nmibnode > 0) {
     const long long nt = (long long)P.nblk[0] + P.nmibnode;
     kf_mib<<<(unsigned)((nt + TPB - 1) / TPB), TPB, 0, st>>>(P, u, d, T.e_next);
     launches++;
   }
-  launch_x_n(P, u, d, T.e_next, st);
+  pass(0, u, d, nullptr, T.e_next);
   mark(1);
   mark(2);
-  launch_yz_n<1, false>(P, d, nullptr, st);
+  pass(1, nullptr, d, nullptr, 0.0);
   mark(3);
   mark(4);
-  launch_yz_n<2, true>(P, d, u, st);
+  pass(2, nullptr, d, u, 0.0);
   mark(5);
   return launches;
 }
