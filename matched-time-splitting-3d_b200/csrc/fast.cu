@@ -21,10 +21,10 @@
 //           all three directions and the jump terms, one thread per node;
 //           the Convert2Tri row operations of the x blocks, one thread per
 //           block, douglas_adi.cc:1554-1675), written into d at those nodes;
-//   kf_xr   rho of the regular x lines (and d on the face lines), fused with
-//           their solves: warp w of a CTA takes one line at a time, the CTA's
-//           warps a 4 (y) x 2 (z) block of lines, so that a line's y and z
-//           neighbours are mostly its siblings' lines and come from L1;
+//   kf_xw   rho of the regular x lines (and d on the face lines), fused with
+//           their solves: a CTA walks a column of planes for TY lines with
+//           the stencil's planes in a shared-memory ring filled by bulk
+//           copies (see the kernel);
 //   kf_xc   the same for the x lines that cross the interface (side stream);
 //   kf_yt   the regular y lines, solved in place on d*, in tiles of NL
 //           neighbouring lines (the same row of NL lines is NL consecutive
@@ -58,8 +58,50 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int YZ_NL = 8;  // lines per tile of kf_yt (one warp each)
-constexpr int XW = 8;     // warps per CTA of kf_xr: a 4 (y) x 2 (z) block of lines
 constexpr int CW = 8;     // warps per CTA of the crossing-line kernels
+constexpr int X_NFACE = 8;  // CTAs of kf_xw that fill the face lines
+constexpr long long kWaitCycles = 1LL << 32;  // ~2 s of SM clock: a bulk copy that has not landed by then never will
+
+// ---------------------------------------------------------------------------
+// Bulk copies into shared memory with mbarrier completion
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// src and dst 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase of the given parity to complete, giving up after
+// kWaitCycles clocks of this SM.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  if (mbar_test(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_test(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+// Orders this thread's generic-proxy shared-memory accesses before later
+// bulk copies into the same memory.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Jump data on the fly (Refresh_Jump, intersection.cc:2294-2490): [u] and
@@ -251,6 +293,49 @@ __device__ __forceinline__ void solve_seg(double* buf, int n, int lane, FI IB, F
   }
 }
 
+// The same with the lane's rows in registers (y: right-hand side in,
+// solution out).
+template <int MX, class FI, class FP, class FQ>
+__device__ __forceinline__ void solve_reg(double (&y)[MX], int n, int lane, FI IB, FP PP, FQ QQ) {
+  const int jb = lane * MX;
+  double B = 0.0, A = 1.0;
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    if (jb + k < n) {
+      const double p = PP(k);
+      y[k] = IB(k) * y[k];
+      B = fma(p, B, y[k]);
+      A *= p;
+    }
+  }
+  double d = carry_up(A, B, lane);
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    if (jb + k < n) {
+      d = fma(PP(k), d, y[k]);
+      y[k] = d;
+    }
+  }
+  B = 0.0;
+  A = 1.0;
+#pragma unroll
+  for (int k = MX - 1; k >= 0; k--) {
+    if (jb + k < n) {
+      const double q = QQ(k);
+      B = fma(q, B, y[k]);
+      A *= q;
+    }
+  }
+  double x = carry_down(A, B, lane);
+#pragma unroll
+  for (int k = MX - 1; k >= 0; k--) {
+    if (jb + k < n) {
+      x = fma(QQ(k), x, y[k]);
+      y[k] = x;
+    }
+  }
+}
+
 // A line without crossings: (ib, p) from the row table of its side in shared
 // memory, tab[0..R) = ib, tab[R..2R) = p, and q = p.
 template <int MX>
@@ -407,65 +492,254 @@ __device__ __forceinline__ void x_rho(const Dev& P, const double* __restrict__ u
   }
 }
 
-template <int MX>
-__host__ __device__ constexpr size_t xr_smem() {
-  // row tables 4 R, one line buffer of R doubles per warp
-  return sizeof(double) * ((size_t)4 * 32 * MX + (size_t)XW * 32 * MX);
+// Shared memory of kf_xw: a ring of 4 slabs of u^n (the TY+2 rows around
+// the CTA's lines at one plane, from a 16-byte aligned start), 4 slabs of
+// their tags (TY rows), sin 2x and x^2 per column, the row tables.
+struct XLayout {
+  int slabd;  // doubles per u^n slab (even)
+  int tagb;   // bytes per tag slab (multiple of 16)
+  size_t o_tag, o_xt, o_tab, o_bar, total;
+};
+__host__ __device__ inline XLayout x_layout(int nx, int TY, int R) {
+  XLayout L;
+  L.slabd = ((TY + 2) * nx + 2 + 1) & ~1;
+  L.tagb = (TY * nx + 32 + 15) & ~15;
+  L.o_tag = (size_t)4 * L.slabd * sizeof(double);
+  L.o_xt = L.o_tag + (size_t)4 * L.tagb;
+  L.o_tab = L.o_xt + (((size_t)2 * nx * sizeof(double) + 15) & ~(size_t)15);
+  L.o_bar = L.o_tab + (size_t)4 * R * sizeof(double);
+  L.total = L.o_bar + 4 * sizeof(uint64_t);
+  return L;
 }
 
-// The regular x lines and the face lines.
-template <int MX>
-__global__ void __launch_bounds__(32 * XW, 4) kf_xr(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                    double* __restrict__ dst, double E) {
+// The x lines that do not cross the interface, and the face lines.  A CTA
+// owns TY neighbouring lines (rows iy0..iy0+TY-1) and walks a range of z
+// planes.  Plane by plane it brings the TY+2 rows of u^n around its lines
+// (one contiguous run of memory) and their tags into shared memory with one
+// bulk copy each (cp.async.bulk, completion on an mbarrier), four planes in a
+// ring, so that the z-1, z and z+1 rows of the stencil all come from shared
+// memory and the copy of plane z+2 is in flight while plane z is computed.
+// Lane l of warp w forms rho of its rows l MX .. l MX + MX - 1 of line
+// iy0 + w in registers; the MIB rows' values (from kf_mib) and the next
+// line's flags are read one plane ahead.  The solved line goes out through
+// the line's z-1 row in shared memory (no other warp reads it) as coalesced
+// stores.
+template <int TY, int MX>
+__global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                    double* __restrict__ dst, double E, int nyt, int zchunk,
+                                                    int ntiles) {
   constexpr int R = 32 * MX;
-  extern __shared__ __align__(16) double smx[];
-  double* const stab = smx;
-  load_tab(stab, P.ftab[0], R);
-  __syncthreads();
   E = step_e(P, E, 2);
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* const buf = smx + 4 * R + w * R;
   const bool eq8 = P.eq != 0;
-  const int nbY = (ny + 3) / 4, nbZ = (nz + 1) / 2;
-  const long long nb = (long long)nbY * nbZ;
-  auto line_of = [&](long long blk, int& iy, int& iz) {
-    iy = (int)(blk % nbY) * 4 + (w & 3);
-    iz = (int)(blk / nbY) * 2 + (w >> 2);
-  };
-  auto flags_of = [&](long long blk) -> int {
-    if (blk >= nb) return 0;
-    int iy, iz;
-    line_of(blk, iy, iz);
-    if (iy >= ny || iz >= nz) return 0;
-    return P.fline[0][(long long)iy * nz + iz];
-  };
-  // the line flags (crossing, side of row 1) are read one line ahead
-  int fl = flags_of(blockIdx.x);
-  for (long long blk = blockIdx.x; blk < nb; blk += gridDim.x) {
-    const int f = fl;
-    fl = flags_of(blk + gridDim.x);
-    int iy, iz;
-    line_of(blk, iy, iz);
-    if (iy >= ny || iz >= nz) continue;  // (warp-uniform)
-    const long long m0 = (long long)nx * (iy + (long long)ny * iz);
-    if (iy == 0 || iz == 0 || iy == ny - 1 || iz == nz - 1) {
-      // face line: d = Outer_u(t_next) - u^n
-      const double yv = P.ax[1][iy], zv = P.ax[2][iz];
-      const double yz2 = yv * yv + zv * zv;
-      for (int j = lane; j < nx; j += 32) {
-        const double x = P.ax[0][j];
-        dst[m0 + j] = (eq8 ? (x * x + yz2) * E : 100.0) - un[m0 + j];
+
+  if ((int)blockIdx.x >= ntiles) {
+    // face x lines (iy or iz on a face): d = Outer_u(t_next) - u^n
+    const int nface = 2 * ny + 2 * (nz - 2);
+    const int fw = (blockIdx.x - ntiles) * TY + w, fstride = (gridDim.x - ntiles) * TY;
+    for (int f = fw; f < nface; f += fstride) {
+      int iy, iz;
+      if (f < 2 * ny) {
+        iy = f % ny;
+        iz = f < ny ? 0 : nz - 1;
+      } else {
+        iz = 1 + (f - 2 * ny) % (nz - 2);
+        iy = (f - 2 * ny) < nz - 2 ? 0 : ny - 1;
       }
-      continue;
+      const long long m0 = (long long)nx * (iy + (long long)ny * iz);
+      const double y = P.ax[1][iy], z = P.ax[2][iz];
+      const double yz2 = y * y + z * z;
+      for (int ix = lane; ix < nx; ix += 32) {
+        const double x = P.ax[0][ix];
+        dst[m0 + ix] = (eq8 ? (x * x + yz2) * E : 100.0) - un[m0 + ix];
+      }
     }
-    if (f & 1) continue;  // crosses the interface: kf_xc
-    x_rho<MX>(P, un, dst, E, iy, iz, buf, lane);
-    __syncwarp();
-    solve_tab<MX>(buf, stab + ((f >> 1) & 1) * 2 * R, nx, lane);
-    __syncwarp();
-    for (int j = lane; j < nx; j += 32) dst[m0 + j] = buf[j];
-    __syncwarp();  // the buffer is free for the next line
+    return;
+  }
+
+  extern __shared__ __align__(16) unsigned char smx[];
+  const XLayout LY = x_layout(nx, TY, R);
+  double* const slab = reinterpret_cast<double*>(smx);
+  unsigned char* const tslab = smx + LY.o_tag;
+  double* const xs2 = reinterpret_cast<double*>(smx + LY.o_xt);  // sin 2x
+  double* const xxx = xs2 + nx;                                   // x^2
+  double* const stab = reinterpret_cast<double*>(smx + LY.o_tab);
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(smx + LY.o_bar);
+
+  const int ty = blockIdx.x % nyt, zc = blockIdx.x / nyt;
+  const int y0 = 1 + ty * TY;
+  const int z0 = 1 + zc * zchunk;
+  const int z1 = min(z0 + zchunk, nz - 1);
+  const int nplanes = z1 - z0;  // >= 1
+  const int nslabs = nplanes + 2;
+
+  // slab i holds plane z0 - 1 + i: where each copy starts, and the offset
+  // (in elements) of the data within the aligned copy
+  auto slab_src = [&](int i, int& shift) -> const double* {
+    const double* g = un + (long long)nx * ((y0 - 1) + (long long)ny * (z0 - 1 + i));
+    const uintptr_t a = reinterpret_cast<uintptr_t>(g);
+    shift = (int)((a & 15) >> 3);
+    return reinterpret_cast<const double*>(a & ~(uintptr_t)15);
+  };
+  auto tag_src = [&](int i, int& shift) -> const unsigned char* {
+    const unsigned char* g = P.tag + (long long)nx * (y0 + (long long)ny * (z0 - 1 + i));
+    const uintptr_t a = reinterpret_cast<uintptr_t>(g);
+    shift = (int)(a & 15);
+    return reinterpret_cast<const unsigned char*>(a & ~(uintptr_t)15);
+  };
+  const unsigned ubytes = (unsigned)((((size_t)(TY + 2) * nx + 1) * sizeof(double) + 15) & ~(size_t)15);
+  const unsigned tbytes = (unsigned)((TY * nx + 15 + 15) & ~15);
+  auto issue = [&](int i) {
+    const int s = i & 3;
+    int sh;
+    const double* gu = slab_src(i, sh);
+    const unsigned char* gt = tag_src(i, sh);
+    mbar_expect(&bar[s], ubytes + tbytes);
+    bulk_copy(slab + (size_t)s * LY.slabd, gu, ubytes, &bar[s]);
+    bulk_copy(tslab + (size_t)s * LY.tagb, gt, tbytes, &bar[s]);
+  };
+  auto tags_of = [&](int i) -> const unsigned char* {  // this warp's tag row of slab i
+    int sh;
+    tag_src(i, sh);
+    return tslab + (size_t)(i & 3) * LY.tagb + sh + (size_t)w * nx;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 4; s++) mbar_init(&bar[s]);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < 3 && i < nslabs; i++) issue(i);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    xs2[i] = P.s2[0][i];
+    const double x = P.ax[0][i];
+    xxx[i] = x * x;
+  }
+  load_tab(stab, P.ftab[0], R);
+  __syncthreads();
+
+  const double cx0 = P.dt * P.vd[0][0][0], cy0 = P.dt * P.vd[1][0][0], cz0 = P.dt * P.vd[2][0][0];
+  const double cx1 = P.dt * P.vd[0][1][0], cy1 = P.dt * P.vd[1][1][0], cz1 = P.dt * P.vd[2][1][0];
+  const int iy = y0 + w;
+  const bool live = iy <= ny - 2;
+  const double yv = P.ax[1][live ? iy : 1];
+  const int jb = lane * MX;
+  const uint8_t* const fl = P.fline[0];
+  // flags of this warp's line at the plane in hand (a line not live, or one
+  // that crosses the interface, is skipped: bit0)
+  int fcur = live ? fl[(long long)iy * nz + z0] : 1;
+  double mcur[MX];  // the MIB rows' values at the plane in hand
+  bool mib_ready = false;
+  bool bad = false;
+
+  for (int pi = 0; pi < nplanes; pi++) {
+    if (threadIdx.x == 0 && pi + 3 < nslabs) issue(pi + 3);
+    const int iz = z0 + pi;
+    // slabs pi (z-1), pi+1 (z), pi+2 (z+1) must have landed
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int i = pi + k;
+      ok = ok && mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
+    }
+    if (!ok) bad = true;
+    const long long m0 = (long long)nx * (iy + (long long)ny * iz);
+    if (ok && !mib_ready && !(fcur & 1)) {
+      // the first plane: its MIB values now (later planes: a plane ahead)
+      const unsigned char* const tg = tags_of(pi + 1);
+#pragma unroll
+      for (int k = 0; k < MX; k++) {
+        const int j = jb + k;
+        mcur[k] = (j > 0 && j < nx - 1 && (tg[j] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) ? dst[m0 + j] : 0.0;
+      }
+    }
+    // the next plane's flags and MIB values, read ahead
+    int fnxt = 1;
+    double mnxt[MX];
+    if (ok && live && pi + 1 < nplanes) {
+      fnxt = fl[(long long)iy * nz + iz + 1];
+      if (!(fnxt & 1)) {
+        const unsigned char* const tg = tags_of(pi + 2);
+        const long long m1 = m0 + (long long)nx * ny;
+#pragma unroll
+        for (int k = 0; k < MX; k++) {
+          const int j = jb + k;
+          mnxt[k] = (j > 0 && j < nx - 1 && (tg[j] & (TAG_MIBX | TAG_MIBY | TAG_MIBZ))) ? dst[m1 + j] : 0.0;
+        }
+      }
+    }
+    if (ok && !(fcur & 1)) {
+      int shm, shc, shp;
+      slab_src(pi, shm);
+      slab_src(pi + 1, shc);
+      slab_src(pi + 2, shp);
+      const double* const sc = slab + (size_t)((pi + 1) & 3) * LY.slabd + shc + (size_t)(w + 1) * nx;
+      const double* const sym = sc - nx;
+      const double* const syp = sc + nx;
+      double* const szm = slab + (size_t)(pi & 3) * LY.slabd + shm + (size_t)(w + 1) * nx;
+      const double* const szp = slab + (size_t)((pi + 2) & 3) * LY.slabd + shp + (size_t)(w + 1) * nx;
+      const unsigned char* const tg = tags_of(pi + 1);
+      const double zv = P.ax[2][iz];
+      const double yz2 = yv * yv + zv * zv;
+      // source constants of the line: inside dt kin sin2x cos2y sin2z E,
+      // outside -dt E (x^2 + y^2 + z^2) - dt 6 beta_out E
+      const double kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
+      const double koa = eq8 ? -P.dt * E : 0.0;
+      const double kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
+      double y[MX];
+#pragma unroll
+      for (int k = 0; k < MX; k++) {
+        const int j = jb + k;
+        double r = 0.0;
+        if (j < nx) {
+          const double uc = sc[j];
+          if (j == 0 || j == nx - 1) {
+            r = (eq8 ? fma(xxx[j], E, yz2 * E) : 100.0) - uc;
+          } else {
+            const int t = tg[j];
+            if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
+              r = mcur[k];
+            } else {
+              const double lx = fma(-2.0, uc, sc[j - 1] + sc[j + 1]);
+              const double ly = fma(-2.0, uc, sym[j] + syp[j]);
+              const double lz = fma(-2.0, uc, szm[j] + szp[j]);
+              if (t & TAG_OUT)
+                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, xxx[j], kob))));
+              else
+                r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * xs2[j])));
+            }
+          }
+        }
+        y[k] = r;
+      }
+      const double* const tab = stab + ((fcur >> 1) & 1) * 2 * R;
+      solve_reg<MX>(
+          y, nx, lane, [&](int k) { return tab[jb + k]; }, [&](int k) { return tab[R + jb + k]; },
+          [&](int k) { return tab[R + jb + k]; });
+      // out through the line's z-1 row (this warp alone reads it, and every
+      // lane is done with it once the solve's shuffles are past)
+#pragma unroll
+      for (int k = 0; k < MX; k++)
+        if (jb + k < nx) szm[jb + k] = y[k];
+      __syncwarp();
+      for (int j = lane; j < nx; j += 32) dst[m0 + j] = szm[j];
+    }
+    fcur = fnxt;
+#pragma unroll
+    for (int k = 0; k < MX; k++) mcur[k] = mnxt[k];
+    mib_ready = true;
+    // every thread's shared-memory accesses to the slot reloaded next are done
+    fence_async_smem();
+    if (__syncthreads_or(bad)) {
+      if (threadIdx.x == 0) {
+        atomicOr(P.status, 2);
+        // let the copies still in flight land before the CTA leaves
+        for (int i = pi + 3; i < nslabs && i < pi + 4; i++) mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
+      }
+      return;
+    }
   }
 }
 
@@ -835,11 +1109,26 @@ int resident_grid(const Dev& P, K kernel, int threads, size_t smem, long long wa
   return (int)std::max(1LL, std::min(want, (long long)per_sm * P.sweep_blocks));
 }
 
+template <int TY, int MX>
+void launch_xw_ty(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
+  const size_t smem = x_layout(P.nx, TY, 32 * MX).total;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_xw<TY, MX>, 32 * TY, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int nyt = (P.ny - 2 + TY - 1) / TY;
+  const int target = std::max(1, per_sm * P.sweep_blocks - X_NFACE);
+  int nzc = std::max(1, std::min(P.nz - 2, target / nyt));
+  const int zchunk = (P.nz - 2 + nzc - 1) / nzc;
+  nzc = (P.nz - 2 + zchunk - 1) / zchunk;
+  const int ntiles = nyt * nzc;
+  kf_xw<TY, MX><<<ntiles + X_NFACE, 32 * TY, smem, st>>>(P, un, d, E, nyt, zchunk, ntiles);
+}
 template <int MX>
 void launch_xr(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  const long long nb = (long long)((P.ny + 3) / 4) * ((P.nz + 1) / 2);
-  const int grid = resident_grid(P, kf_xr<MX>, 32 * XW, xr_smem<MX>(), nb);
-  kf_xr<MX><<<grid, 32 * XW, xr_smem<MX>(), st>>>(P, un, d, E);
+  if (x_layout(P.nx, 8, 32 * MX).total <= (size_t)113 * 1024)
+    launch_xw_ty<8, MX>(P, un, d, E, st);
+  else
+    launch_xw_ty<4, MX>(P, un, d, E, st);
 }
 template <int MX>
 void launch_xc(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
@@ -885,7 +1174,8 @@ void launch_dir(const Dev& P, int d, bool crossing, const double* un, double* f,
 
 template <int MX>
 void fast_attr() {
-  cudaFuncSetAttribute(kf_xr<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem<MX>());
+  cudaFuncSetAttribute(kf_xw<8, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSweepSmem);
+  cudaFuncSetAttribute(kf_xw<4, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSweepSmem);
   cudaFuncSetAttribute(kf_xc<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
   cudaFuncSetAttribute(kf_yt<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)yt_smem<MX, false>());
@@ -904,7 +1194,10 @@ void configure_fast_kernels() {
 
 int fast_rows_per_lane(int n) { return fast_mx(n); }
 
-bool fast_fits(int nx, int ny, int nz) { return fast_mx(nx) && fast_mx(ny) && fast_mx(nz); }
+bool fast_fits(int nx, int ny, int nz) {
+  const int mx = fast_mx(nx);
+  return mx && fast_mx(ny) && fast_mx(nz) && x_layout(nx, 4, 32 * mx).total <= (size_t)kMaxSweepSmem;
+}
 
 int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t st) {
   kf_fline<0><<<(unsigned)((nlines<0>(P) + TPB - 1) / TPB), TPB, 0, st>>>(P, fline[0]);
