@@ -245,7 +245,11 @@ mts_status mts_autotune(mts_handle h, int32_t steps, int32_t shapes[3]);
  * line is solved by one warp whose lanes split the Thomas recurrences into
  * segments joined by shuffle scans.  The operations are those of the plain
  * form in another order, so results differ from it by rounding only (within
- * 1e-10 relative max-norm over the runs the tests cover).  Switching it on
+ * 1e-10 relative max-norm over the runs the tests cover).  Where setup has
+ * reported near-singular MIB weight systems (mts_get_counts()[7] > 0) the
+ * problem itself is that sensitive to rounding (the reference's own code
+ * moves by ~1e-5 when compiled with fused multiply-adds) and only the plain
+ * form reproduces the reference to 1e-10.  Switching it on
  * builds its row tables and, for each line that crosses the interface, its
  * per-row solve coefficients (3 x 8 bytes per row) on the device once.
  * Profiling slots of this form: {0 MIB rows + residual + x solve, 1 y solve,
