@@ -1180,9 +1180,15 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
         std::vector<uint8_t> hf(nl);
         CUDA_TRY(cudaMemcpyAsync(hf.data(), fl[d], nl, cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
+        // listed in memory order (the fast line index first), so that the
+        // warps that take neighbouring entries read neighbouring lines
+        const int n1 = d == 0 ? h->g.ny : h->g.nx, n2 = d == 2 ? h->g.ny : h->g.nz;
         std::vector<int32_t> list;
-        for (size_t l = 0; l < nl; l++)
-          if (hf[l] & 1) list.push_back((int32_t)l);
+        for (int i2 = 0; i2 < n2; i2++)
+          for (int i1 = 0; i1 < n1; i1++) {
+            const size_t l = (size_t)i1 * n2 + i2;
+            if (hf[l] & 1) list.push_back((int32_t)l);
+          }
         int32_t* dl = nullptr;
         double *cf = nullptr, *bq = nullptr;
         if (!list.empty()) {

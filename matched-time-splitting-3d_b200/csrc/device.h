@@ -125,7 +125,7 @@ struct Dev {
   // switched on.  Per direction: the row tables [side][1/bet, -a/bet][32 MX]
   // of the lines without crossings; per line a flag byte (bit0 the line
   // crosses the interface, bit1 the side of its row 1); the crossing lines'
-  // ids in line order (fcross, nfcross of them) and their own rows
+  // ids in memory order (fcross, nfcross of them) and their own rows
   // [c][1/bet, -a/bet][32 MX]; per block the -gam_{j+1} of its rows.  Per
   // MIB node its block in x, y, z (-1: none); per x block the MIB node
   // index of each of its rows.

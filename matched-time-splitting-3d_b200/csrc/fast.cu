@@ -492,23 +492,23 @@ __device__ __forceinline__ void x_rho(const Dev& P, const double* __restrict__ u
   }
 }
 
-// Shared memory of kf_xw: a ring of 4 slabs of u^n (the TY+2 rows around
-// the CTA's lines at one plane, from a 16-byte aligned start), 4 slabs of
-// their tags (TY rows), sin 2x and x^2 per column, the row tables.
+// Shared memory of kf_xw: a ring of XS slabs of u^n (the TY+2 rows around
+// the CTA's lines at one plane, from a 16-byte aligned start) and XS slabs
+// of their tags (TY rows).  Three slabs are in use at a plane (z-1, z, z+1)
+// and two more are on their way.
+constexpr int XS = 5;
 struct XLayout {
   int slabd;  // doubles per u^n slab (even)
   int tagb;   // bytes per tag slab (multiple of 16)
-  size_t o_tag, o_xt, o_tab, o_bar, total;
+  size_t o_tag, o_bar, total;
 };
-__host__ __device__ inline XLayout x_layout(int nx, int TY, int R) {
+__host__ __device__ inline XLayout x_layout(int nx, int TY) {
   XLayout L;
   L.slabd = ((TY + 2) * nx + 2 + 1) & ~1;
   L.tagb = (TY * nx + 32 + 15) & ~15;
-  L.o_tag = (size_t)4 * L.slabd * sizeof(double);
-  L.o_xt = L.o_tag + (size_t)4 * L.tagb;
-  L.o_tab = L.o_xt + (((size_t)2 * nx * sizeof(double) + 15) & ~(size_t)15);
-  L.o_bar = L.o_tab + (size_t)4 * R * sizeof(double);
-  L.total = L.o_bar + 4 * sizeof(uint64_t);
+  L.o_tag = (size_t)XS * L.slabd * sizeof(double);
+  L.o_bar = L.o_tag + (size_t)XS * L.tagb;
+  L.total = L.o_bar + XS * sizeof(uint64_t);
   return L;
 }
 
@@ -516,9 +516,11 @@ __host__ __device__ inline XLayout x_layout(int nx, int TY, int R) {
 // owns TY neighbouring lines (rows iy0..iy0+TY-1) and walks a range of z
 // planes.  Plane by plane it brings the TY+2 rows of u^n around its lines
 // (one contiguous run of memory) and their tags into shared memory with one
-// bulk copy each (cp.async.bulk, completion on an mbarrier), four planes in a
+// bulk copy each (cp.async.bulk, completion on an mbarrier), XS planes in a
 // ring, so that the z-1, z and z+1 rows of the stencil all come from shared
-// memory and the copy of plane z+2 is in flight while plane z is computed.
+// memory and the copies of planes z+2 and z+3 are in flight while plane z is
+// computed.  The row tables and the per-column sin 2x, x^2 are read through
+// L1.
 // Lane l of warp w forms rho of its rows l MX .. l MX + MX - 1 of line
 // iy0 + w in registers; the MIB rows' values (from kf_mib) and the next
 // line's flags are read one plane ahead.  The solved line goes out through
@@ -559,13 +561,13 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   }
 
   extern __shared__ __align__(16) unsigned char smx[];
-  const XLayout LY = x_layout(nx, TY, R);
+  const XLayout LY = x_layout(nx, TY);
   double* const slab = reinterpret_cast<double*>(smx);
   unsigned char* const tslab = smx + LY.o_tag;
-  double* const xs2 = reinterpret_cast<double*>(smx + LY.o_xt);  // sin 2x
-  double* const xxx = xs2 + nx;                                   // x^2
-  double* const stab = reinterpret_cast<double*>(smx + LY.o_tab);
   uint64_t* const bar = reinterpret_cast<uint64_t*>(smx + LY.o_bar);
+  const double* __restrict__ const xs2 = P.s2[0];  // sin 2x
+  const double* __restrict__ const xa = P.ax[0];   // x
+  const double* __restrict__ const stab = P.ftab[0];
 
   const int ty = blockIdx.x % nyt, zc = blockIdx.x / nyt;
   const int y0 = 1 + ty * TY;
@@ -591,7 +593,7 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   const unsigned ubytes = (unsigned)((((size_t)(TY + 2) * nx + 1) * sizeof(double) + 15) & ~(size_t)15);
   const unsigned tbytes = (unsigned)((TY * nx + 15 + 15) & ~15);
   auto issue = [&](int i) {
-    const int s = i & 3;
+    const int s = i % XS;
     int sh;
     const double* gu = slab_src(i, sh);
     const unsigned char* gt = tag_src(i, sh);
@@ -602,23 +604,16 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   auto tags_of = [&](int i) -> const unsigned char* {  // this warp's tag row of slab i
     int sh;
     tag_src(i, sh);
-    return tslab + (size_t)(i & 3) * LY.tagb + sh + (size_t)w * nx;
+    return tslab + (size_t)(i % XS) * LY.tagb + sh + (size_t)w * nx;
   };
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 4; s++) mbar_init(&bar[s]);
+    for (int s = 0; s < XS; s++) mbar_init(&bar[s]);
     mbar_init_fence();
   }
   __syncthreads();
   if (threadIdx.x == 0)
-    for (int i = 0; i < 3 && i < nslabs; i++) issue(i);
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    xs2[i] = P.s2[0][i];
-    const double x = P.ax[0][i];
-    xxx[i] = x * x;
-  }
-  load_tab(stab, P.ftab[0], R);
-  __syncthreads();
+    for (int i = 0; i < XS - 1 && i < nslabs; i++) issue(i);
 
   const double cx0 = P.dt * P.vd[0][0][0], cy0 = P.dt * P.vd[1][0][0], cz0 = P.dt * P.vd[2][0][0];
   const double cx1 = P.dt * P.vd[0][1][0], cy1 = P.dt * P.vd[1][1][0], cz1 = P.dt * P.vd[2][1][0];
@@ -635,14 +630,16 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   bool bad = false;
 
   for (int pi = 0; pi < nplanes; pi++) {
-    if (threadIdx.x == 0 && pi + 3 < nslabs) issue(pi + 3);
+    // (slab pi + XS - 1 goes into the slot of slab pi - 1, done with at the
+    // last plane)
+    if (threadIdx.x == 0 && pi + XS - 1 < nslabs) issue(pi + XS - 1);
     const int iz = z0 + pi;
     // slabs pi (z-1), pi+1 (z), pi+2 (z+1) must have landed
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const int i = pi + k;
-      ok = ok && mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
+      ok = ok && mbar_wait(&bar[i % XS], (unsigned)((i / XS) & 1));
     }
     if (!ok) bad = true;
     const long long m0 = (long long)nx * (iy + (long long)ny * iz);
@@ -675,11 +672,11 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
       slab_src(pi, shm);
       slab_src(pi + 1, shc);
       slab_src(pi + 2, shp);
-      const double* const sc = slab + (size_t)((pi + 1) & 3) * LY.slabd + shc + (size_t)(w + 1) * nx;
+      const double* const sc = slab + (size_t)((pi + 1) % XS) * LY.slabd + shc + (size_t)(w + 1) * nx;
       const double* const sym = sc - nx;
       const double* const syp = sc + nx;
-      double* const szm = slab + (size_t)(pi & 3) * LY.slabd + shm + (size_t)(w + 1) * nx;
-      const double* const szp = slab + (size_t)((pi + 2) & 3) * LY.slabd + shp + (size_t)(w + 1) * nx;
+      double* const szm = slab + (size_t)(pi % XS) * LY.slabd + shm + (size_t)(w + 1) * nx;
+      const double* const szp = slab + (size_t)((pi + 2) % XS) * LY.slabd + shp + (size_t)(w + 1) * nx;
       const unsigned char* const tg = tags_of(pi + 1);
       const double zv = P.ax[2][iz];
       const double yz2 = yv * yv + zv * zv;
@@ -695,8 +692,9 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
         double r = 0.0;
         if (j < nx) {
           const double uc = sc[j];
+          const double x = xa[j];
           if (j == 0 || j == nx - 1) {
-            r = (eq8 ? fma(xxx[j], E, yz2 * E) : 100.0) - uc;
+            r = (eq8 ? fma(x * x, E, yz2 * E) : 100.0) - uc;
           } else {
             const int t = tg[j];
             if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
@@ -706,7 +704,7 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
               const double ly = fma(-2.0, uc, sym[j] + syp[j]);
               const double lz = fma(-2.0, uc, szm[j] + szp[j]);
               if (t & TAG_OUT)
-                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, xxx[j], kob))));
+                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, x * x, kob))));
               else
                 r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * xs2[j])));
             }
@@ -736,7 +734,7 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
       if (threadIdx.x == 0) {
         atomicOr(P.status, 2);
         // let the copies still in flight land before the CTA leaves
-        for (int i = pi + 3; i < nslabs && i < pi + 4; i++) mbar_wait(&bar[i & 3], (unsigned)((i >> 2) & 1));
+        for (int i = pi + 3; i < nslabs && i < pi + XS; i++) mbar_wait(&bar[i % XS], (unsigned)((i / XS) & 1));
       }
       return;
     }
@@ -1111,7 +1109,7 @@ int resident_grid(const Dev& P, K kernel, int threads, size_t smem, long long wa
 
 template <int TY, int MX>
 void launch_xw_ty(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  const size_t smem = x_layout(P.nx, TY, 32 * MX).total;
+  const size_t smem = x_layout(P.nx, TY).total;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_xw<TY, MX>, 32 * TY, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1125,7 +1123,7 @@ void launch_xw_ty(const Dev& P, const double* un, double* d, double E, cudaStrea
 }
 template <int MX>
 void launch_xr(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  if (x_layout(P.nx, 8, 32 * MX).total <= (size_t)113 * 1024)
+  if (x_layout(P.nx, 8).total <= (size_t)113 * 1024)
     launch_xw_ty<8, MX>(P, un, d, E, st);
   else
     launch_xw_ty<4, MX>(P, un, d, E, st);
@@ -1196,7 +1194,7 @@ int fast_rows_per_lane(int n) { return fast_mx(n); }
 
 bool fast_fits(int nx, int ny, int nz) {
   const int mx = fast_mx(nx);
-  return mx && fast_mx(ny) && fast_mx(nz) && x_layout(nx, 4, 32 * mx).total <= (size_t)kMaxSweepSmem;
+  return mx && fast_mx(ny) && fast_mx(nz) && x_layout(nx, 4).total <= (size_t)kMaxSweepSmem;
 }
 
 int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t st) {
