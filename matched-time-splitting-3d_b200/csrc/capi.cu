@@ -1167,7 +1167,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
       for (int d = 0; d < 3; d++) {
         const size_t R = 32 * (size_t)mts::fast_rows_per_lane(nd[d]);
         double* tab = nullptr;
-        CUDA_TRY(h->put(&tab, (const double*)nullptr, 4 * R));
+        CUDA_TRY(h->put(&tab, (const double*)nullptr, 2 * (2 * R + 320)));
         D.ftab[d] = tab;
         CUDA_TRY(h->put(&fl[d], (const uint8_t*)nullptr, (size_t)line_count(h->g, d)));
         D.fline[d] = fl[d];

@@ -122,8 +122,9 @@ struct Dev {
   float* ctab[3];
   int precision;              // 0 plain FP64, 1 mixed, 2 fast FP64
   // Fast FP64 form (segmented line solves, fast.cu), built when the form is
-  // switched on.  Per direction: the row tables [side][1/bet, -a/bet][32 MX]
-  // of the lines without crossings; per line a flag byte (bit0 the line
+  // switched on.  Per direction: the row tables [side][1/bet, -a/bet by row
+  // (32 MX each), then 2 x 5 x 32 lane-scan multipliers] of the lines
+  // without crossings; per line a flag byte (bit0 the line
   // crosses the interface, bit1 the side of its row 1); the crossing lines'
   // ids in memory order (fcross, nfcross of them) and their own rows
   // [c][1/bet, -a/bet][32 MX]; per block the -gam_{j+1} of its rows.  Per

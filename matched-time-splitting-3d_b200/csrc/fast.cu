@@ -336,15 +336,76 @@ __device__ __forceinline__ void solve_reg(double (&y)[MX], int n, int lane, FI I
   }
 }
 
-// A line without crossings: (ib, p) from the row table of its side in shared
-// memory, tab[0..R) = ib, tab[R..2R) = p, and q = p.
+// Row table of one side of a direction, TABW(MX) doubles: ib[R], p[R] by
+// row, then the multipliers of the two lane scans, fm[5][32] and bm[5][32].
+// With q = p on every row of such a line, a lane's forward end map is
+// c -> A c + B and its backward one X -> A X + B', with the same A (the
+// product of its rows' p); step s of the Kogge-Stone scan over the lanes
+// multiplies the value shuffled in from 2^s lanes away by the product of A
+// over the lane's current window: fm[s][l] = prod A over (l - 2^s, l] (0
+// when l < 2^s), bm[s][l] = prod A over [l, l + 2^s) (0 past lane 31).
+// Those are constants of the side, so a scan step is two shuffles and one
+// fused multiply-add.
 template <int MX>
-__device__ __forceinline__ void solve_tab(double* buf, const double* tab, int n, int lane) {
+__host__ __device__ constexpr int tabw() {
+  return 2 * 32 * MX + 320;
+}
+
+// The lane's rows of a line without crossings, in registers (y: right-hand
+// side in, solution out; rows past the line end must hold 0).
+template <int MX>
+__device__ __forceinline__ void solve_lean(double (&y)[MX], const double* tab, int lane) {
   constexpr int R = 32 * MX;
   const int jb = lane * MX;
-  solve_seg<MX>(
-      buf, n, lane, [&](int k) { return tab[jb + k]; }, [&](int k) { return tab[R + jb + k]; },
-      [&](int k) { return tab[R + jb + k]; });
+  const double* const fm = tab + 2 * R;
+  const double* const bm = fm + 160;
+  double p[MX];
+  double B = 0.0;
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    p[k] = tab[R + jb + k];
+    y[k] *= tab[jb + k];
+    B = fma(p[k], B, y[k]);
+  }
+#pragma unroll
+  for (int st = 0; st < 5; st++) {
+    const double Bp = __shfl_up_sync(FULL, B, 1 << st);
+    B = fma(fm[32 * st + lane], Bp, B);
+  }
+  double d = __shfl_up_sync(FULL, B, 1);
+  if (lane == 0) d = 0.0;
+#pragma unroll
+  for (int k = 0; k < MX; k++) {
+    d = fma(p[k], d, y[k]);
+    y[k] = d;
+  }
+  B = 0.0;
+#pragma unroll
+  for (int k = MX - 1; k >= 0; k--) B = fma(p[k], B, y[k]);
+#pragma unroll
+  for (int st = 0; st < 5; st++) {
+    const double Bp = __shfl_down_sync(FULL, B, 1 << st);
+    B = fma(bm[32 * st + lane], Bp, B);
+  }
+  double x = __shfl_down_sync(FULL, B, 1);
+  if (lane == 31) x = 0.0;
+#pragma unroll
+  for (int k = MX - 1; k >= 0; k--) {
+    x = fma(p[k], x, y[k]);
+    y[k] = x;
+  }
+}
+
+// The same on a line held in shared memory (rows past the end hold 0).
+template <int MX>
+__device__ __forceinline__ void solve_tab(double* buf, const double* tab, int lane) {
+  const int jb = lane * MX;
+  double y[MX];
+#pragma unroll
+  for (int k = 0; k < MX; k++) y[k] = buf[jb + k];
+  solve_lean<MX>(y, tab, lane);
+#pragma unroll
+  for (int k = 0; k < MX; k++) buf[jb + k] = y[k];
 }
 
 // A line that crosses the interface: the lane's rows of its own coefficients
@@ -377,9 +438,9 @@ __device__ __forceinline__ void solve_cross(double* buf, const double* qbuf, con
       [&](int k) { return qbuf[jb + k]; });
 }
 
-// Row tables [side][ib, p][R] into shared memory.
-__device__ __forceinline__ void load_tab(double* s, const double* g, int R) {
-  for (int i = threadIdx.x; i < 4 * R; i += blockDim.x) s[i] = g[i];
+// Row tables [side][TABW] into shared memory.
+__device__ __forceinline__ void load_tab(double* s, const double* g, int w2) {
+  for (int i = threadIdx.x; i < w2; i += blockDim.x) s[i] = g[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -494,20 +555,22 @@ __device__ __forceinline__ void x_rho(const Dev& P, const double* __restrict__ u
 
 // Shared memory of kf_xw: a ring of XS slabs of u^n (the TY+2 rows around
 // the CTA's lines at one plane, from a 16-byte aligned start) and XS slabs
-// of their tags (TY rows).  Three slabs are in use at a plane (z-1, z, z+1)
-// and two more are on their way.
-constexpr int XS = 5;
+// of their tags (TY rows), {sin 2x, x^2} per column, the row tables.  Three
+// slabs are in use at a plane (z-1, z, z+1) and one more is on its way.
+constexpr int XS = 4;
 struct XLayout {
   int slabd;  // doubles per u^n slab (even)
   int tagb;   // bytes per tag slab (multiple of 16)
-  size_t o_tag, o_bar, total;
+  size_t o_tag, o_xt, o_tab, o_bar, total;
 };
-__host__ __device__ inline XLayout x_layout(int nx, int TY) {
+__host__ __device__ inline XLayout x_layout(int nx, int TY, int MX) {
   XLayout L;
   L.slabd = ((TY + 2) * nx + 2 + 1) & ~1;
   L.tagb = (TY * nx + 32 + 15) & ~15;
   L.o_tag = (size_t)XS * L.slabd * sizeof(double);
-  L.o_bar = L.o_tag + (size_t)XS * L.tagb;
+  L.o_xt = L.o_tag + (size_t)XS * L.tagb;
+  L.o_tab = L.o_xt + (size_t)(nx + 1) * 2 * sizeof(double);
+  L.o_bar = L.o_tab + (size_t)2 * (2 * 32 * MX + 320) * sizeof(double);
   L.total = L.o_bar + XS * sizeof(uint64_t);
   return L;
 }
@@ -518,9 +581,7 @@ __host__ __device__ inline XLayout x_layout(int nx, int TY) {
 // (one contiguous run of memory) and their tags into shared memory with one
 // bulk copy each (cp.async.bulk, completion on an mbarrier), XS planes in a
 // ring, so that the z-1, z and z+1 rows of the stencil all come from shared
-// memory and the copies of planes z+2 and z+3 are in flight while plane z is
-// computed.  The row tables and the per-column sin 2x, x^2 are read through
-// L1.
+// memory and the copy of plane z+2 is in flight while plane z is computed.
 // Lane l of warp w forms rho of its rows l MX .. l MX + MX - 1 of line
 // iy0 + w in registers; the MIB rows' values (from kf_mib) and the next
 // line's flags are read one plane ahead.  The solved line goes out through
@@ -561,13 +622,12 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   }
 
   extern __shared__ __align__(16) unsigned char smx[];
-  const XLayout LY = x_layout(nx, TY);
+  const XLayout LY = x_layout(nx, TY, MX);
   double* const slab = reinterpret_cast<double*>(smx);
   unsigned char* const tslab = smx + LY.o_tag;
+  double2* const xt = reinterpret_cast<double2*>(smx + LY.o_xt);  // {sin 2x, x^2} per column
+  double* const stab = reinterpret_cast<double*>(smx + LY.o_tab);
   uint64_t* const bar = reinterpret_cast<uint64_t*>(smx + LY.o_bar);
-  const double* __restrict__ const xs2 = P.s2[0];  // sin 2x
-  const double* __restrict__ const xa = P.ax[0];   // x
-  const double* __restrict__ const stab = P.ftab[0];
 
   const int ty = blockIdx.x % nyt, zc = blockIdx.x / nyt;
   const int y0 = 1 + ty * TY;
@@ -614,6 +674,12 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
   __syncthreads();
   if (threadIdx.x == 0)
     for (int i = 0; i < XS - 1 && i < nslabs; i++) issue(i);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const double x = P.ax[0][i];
+    xt[i] = make_double2(P.s2[0][i], x * x);
+  }
+  load_tab(stab, P.ftab[0], 2 * tabw<MX>());
+  __syncthreads();
 
   const double cx0 = P.dt * P.vd[0][0][0], cy0 = P.dt * P.vd[1][0][0], cz0 = P.dt * P.vd[2][0][0];
   const double cx1 = P.dt * P.vd[0][1][0], cy1 = P.dt * P.vd[1][1][0], cz1 = P.dt * P.vd[2][1][0];
@@ -685,37 +751,41 @@ __global__ void __launch_bounds__(32 * TY, 2) kf_xw(const __grid_constant__ Dev 
       const double kin = eq8 ? P.dt * (P.kin * ((P.c2[1][iy] * P.s2[2][iz]) * E)) : 0.0;
       const double koa = eq8 ? -P.dt * E : 0.0;
       const double kob = eq8 ? -P.dt * E * yz2 - P.dt * (P.c6bo * E) : 0.0;
+      // the lane's rows and the two beside them: x +- 1 from registers
+      double uc[MX + 2];
+#pragma unroll
+      for (int k = 0; k < MX + 2; k++) {
+        const int j = jb + k - 1;
+        uc[k] = (j >= 0 && j < nx) ? sc[j] : 0.0;
+      }
       double y[MX];
 #pragma unroll
       for (int k = 0; k < MX; k++) {
         const int j = jb + k;
         double r = 0.0;
         if (j < nx) {
-          const double uc = sc[j];
-          const double x = xa[j];
+          const double2 q = xt[j];
           if (j == 0 || j == nx - 1) {
-            r = (eq8 ? fma(x * x, E, yz2 * E) : 100.0) - uc;
+            r = (eq8 ? fma(q.y, E, yz2 * E) : 100.0) - uc[k + 1];
           } else {
             const int t = tg[j];
             if (t & (TAG_MIBX | TAG_MIBY | TAG_MIBZ)) {
               r = mcur[k];
             } else {
-              const double lx = fma(-2.0, uc, sc[j - 1] + sc[j + 1]);
-              const double ly = fma(-2.0, uc, sym[j] + syp[j]);
-              const double lz = fma(-2.0, uc, szm[j] + szp[j]);
+              const double c0 = uc[k + 1];
+              const double lx = fma(-2.0, c0, uc[k] + uc[k + 2]);
+              const double ly = fma(-2.0, c0, sym[j] + syp[j]);
+              const double lz = fma(-2.0, c0, szm[j] + szp[j]);
               if (t & TAG_OUT)
-                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, x * x, kob))));
+                r = fma(cx1, lx, fma(cy1, ly, fma(cz1, lz, fma(koa, q.y, kob))));
               else
-                r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * xs2[j])));
+                r = fma(cx0, lx, fma(cy0, ly, fma(cz0, lz, kin * q.x)));
             }
           }
         }
         y[k] = r;
       }
-      const double* const tab = stab + ((fcur >> 1) & 1) * 2 * R;
-      solve_reg<MX>(
-          y, nx, lane, [&](int k) { return tab[jb + k]; }, [&](int k) { return tab[R + jb + k]; },
-          [&](int k) { return tab[R + jb + k]; });
+      solve_lean<MX>(y, stab + ((fcur >> 1) & 1) * tabw<MX>(), lane);
       // out through the line's z-1 row (this warp alone reads it, and every
       // lane is done with it once the solve's shuffles are past)
 #pragma unroll
@@ -783,9 +853,9 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_xc(const __grid_constant__ Dev 
 
 template <int MX, bool ACC>
 __host__ __device__ constexpr size_t yt_smem() {
-  // row tables 4 R; two buffers of NL lines x (R + 1) doubles; ACC: one
+  // row tables 2 TABW; two buffers of NL lines x (R + 2) doubles; ACC: one
   // buffer of u^n
-  return sizeof(double) * ((size_t)4 * 32 * MX + (size_t)(ACC ? 3 : 2) * YZ_NL * (32 * MX + 1));
+  return sizeof(double) * ((size_t)2 * tabw<MX>() + (size_t)(ACC ? 3 : 2) * YZ_NL * (32 * MX + 2));
 }
 
 // The regular lines of direction D in tiles: y in place on d*; z (ACC) with
@@ -796,10 +866,12 @@ __global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_co
                                                                   int ntiles) {
   static_assert(D == 1 || D == 2, "y and z lines");
   constexpr int R = 32 * MX;
-  constexpr int LS = R + 1;  // odd: a copy's lines and a lane's stride-MX rows fall on distinct banks
+  // line stride 2 mod 16 doubles: the 8 lines x 2 rows of a half-warp's copy
+  // fall on distinct bank pairs, as do a lane's stride-MX rows (MX odd)
+  constexpr int LS = R + 2;
   extern __shared__ __align__(16) double smyz[];
   double* const stab = smyz;
-  double* const bufs = smyz + 4 * R;
+  double* const bufs = smyz + 2 * tabw<MX>();
   double* const ubuf = bufs + 2 * YZ_NL * LS;  // (ACC)
   const int nx = P.nx;
   const int n = D == 1 ? P.ny : P.nz;
@@ -815,7 +887,10 @@ __global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_co
   const int c = threadIdx.x % YZ_NL, jc = threadIdx.x / YZ_NL;  // this thread's copy share: line c, rows jc + 32 m
   const uint8_t* const fline = P.fline[D];
 
-  load_tab(stab, P.ftab[D], R);
+  load_tab(stab, P.ftab[D], 2 * tabw<MX>());
+  // the rows past the line end stay 0 (the copies never write them)
+  for (int i = threadIdx.x; i < 2 * YZ_NL * LS; i += blockDim.x) bufs[i] = 0.0;
+  __syncthreads();
 
   struct Tile {
     int i1, i2;
@@ -870,7 +945,7 @@ __global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_co
     {
       const int i1 = cur.i1 + w;
       const bool interior = i1 >= 1 && i1 <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
-      if (fw0 >= 0 && !(fw0 & 1) && interior) solve_tab<MX>(buf + w * LS, stab + ((fw0 >> 1) & 1) * 2 * R, n, lane);
+      if (fw0 >= 0 && !(fw0 & 1) && interior) solve_tab<MX>(buf + w * LS, stab + ((fw0 >> 1) & 1) * tabw<MX>(), lane);
     }
     if (ACC) cp_async_wait<1>();
     __syncthreads();
@@ -955,8 +1030,8 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_yc(const __grid_constant__ Dev 
 // ---------------------------------------------------------------------------
 // Set-up of the form (once per handle).
 
-// Row tables of direction D: [side][ib, p][R] from the prefix factors of
-// that side (ptab: bet_j, gam_j); zero past the line end.
+// Row tables of direction D: [side][TABW]: ib and p by row from the prefix
+// factors of that side (ptab: bet_j, gam_j), zero past the line end.
 template <int D>
 __global__ void __launch_bounds__(TPB) kf_tab(const __grid_constant__ Dev P, double* tab, int R) {
   const int n = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
@@ -970,9 +1045,40 @@ __global__ void __launch_bounds__(TPB) kf_tab(const __grid_constant__ Dev P, dou
     ib = 1.0 / bet;
     p = -(a / bet);
   }
-  double* T = tab + (size_t)side * 2 * R;
+  double* T = tab + (size_t)side * (2 * R + 320);
   T[j] = ib;
   T[R + j] = p;
+}
+
+// The scan multipliers of the row tables (after kf_tab), one thread per side.
+__global__ void kf_tabscan(double* tab, int R, int n) {
+  const int side = threadIdx.x;
+  if (side >= 2) return;
+  double* T = tab + (size_t)side * (2 * R + 320);
+  const int MX = R / 32;
+  double A[32];
+  for (int l = 0; l < 32; l++) {
+    double a = 1.0;
+    for (int k = 0; k < MX; k++)
+      if (l * MX + k < n) a *= T[R + l * MX + k];
+    A[l] = a;
+  }
+  for (int st = 0; st < 5; st++) {
+    const int o = 1 << st;
+    for (int l = 0; l < 32; l++) {
+      double f = 0.0, b = 0.0;
+      if (l >= o) {
+        f = 1.0;
+        for (int m = l - o + 1; m <= l; m++) f *= A[m];
+      }
+      if (l + o <= 31) {
+        b = 1.0;
+        for (int m = l; m < l + o; m++) b *= A[m];
+      }
+      T[2 * R + 32 * st + l] = f;
+      T[2 * R + 160 + 32 * st + l] = b;
+    }
+  }
 }
 
 // Per line of direction D: bit0 the line crosses the interface (has MIB
@@ -1109,7 +1215,7 @@ int resident_grid(const Dev& P, K kernel, int threads, size_t smem, long long wa
 
 template <int TY, int MX>
 void launch_xw_ty(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  const size_t smem = x_layout(P.nx, TY).total;
+  const size_t smem = x_layout(P.nx, TY, MX).total;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_xw<TY, MX>, 32 * TY, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1123,7 +1229,7 @@ void launch_xw_ty(const Dev& P, const double* un, double* d, double E, cudaStrea
 }
 template <int MX>
 void launch_xr(const Dev& P, const double* un, double* d, double E, cudaStream_t st) {
-  if (x_layout(P.nx, 8).total <= (size_t)113 * 1024)
+  if (x_layout(P.nx, 8, MX).total <= (size_t)113 * 1024)
     launch_xw_ty<8, MX>(P, un, d, E, st);
   else
     launch_xw_ty<4, MX>(P, un, d, E, st);
@@ -1194,7 +1300,7 @@ int fast_rows_per_lane(int n) { return fast_mx(n); }
 
 bool fast_fits(int nx, int ny, int nz) {
   const int mx = fast_mx(nx);
-  return mx && fast_mx(ny) && fast_mx(nz) && x_layout(nx, 4).total <= (size_t)kMaxSweepSmem;
+  return mx && fast_mx(ny) && fast_mx(nz) && x_layout(nx, 4, mx).total <= (size_t)kMaxSweepSmem;
 }
 
 int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t st) {
@@ -1214,7 +1320,8 @@ int build_fast_tables(const Dev& P, cudaStream_t st) {
     if (d == 0) kf_tab<0><<<g, TPB, 0, st>>>(P, tab, R);
     if (d == 1) kf_tab<1><<<g, TPB, 0, st>>>(P, tab, R);
     if (d == 2) kf_tab<2><<<g, TPB, 0, st>>>(P, tab, R);
-    launches++;
+    kf_tabscan<<<1, 32, 0, st>>>(tab, R, nd[d]);
+    launches += 2;
     if (P.nblk[d] == 0) continue;
     double* cf = const_cast<double*>(P.fcoef[d]);
     double* bq = const_cast<double*>(P.fbq[d]);
