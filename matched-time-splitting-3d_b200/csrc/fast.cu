@@ -57,7 +57,7 @@ namespace mts {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int YZ_NL = 8;  // lines per tile of kf_yt (one warp each)
+constexpr int YZ_NL = 16;  // lines per tile of kf_yt (one warp each): rows of 128 bytes
 constexpr int CW = 8;     // warps per CTA of the crossing-line kernels
 constexpr int X_NFACE = 8;  // CTAs of kf_xw that fill the face lines
 constexpr long long kWaitCycles = 1LL << 32;  // ~2 s of SM clock: a bulk copy that has not landed by then never will
@@ -861,13 +861,13 @@ __host__ __device__ constexpr size_t yt_smem() {
 // The regular lines of direction D in tiles: y in place on d*; z (ACC) with
 // the update of u, face lines included (their d** passes through).
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_constant__ Dev P,
+__global__ void __launch_bounds__(32 * YZ_NL, ACC ? 1 : 2) kf_yt(const __grid_constant__ Dev P,
                                                                   double* __restrict__ f, double* __restrict__ u,
                                                                   int ntiles) {
   static_assert(D == 1 || D == 2, "y and z lines");
   constexpr int R = 32 * MX;
-  // line stride 2 mod 16 doubles: the 8 lines x 2 rows of a half-warp's copy
-  // fall on distinct bank pairs, as do a lane's stride-MX rows (MX odd)
+  // line stride 2 mod 16 doubles: a lane's stride-MX rows (MX odd) fall on
+  // distinct bank pairs
   constexpr int LS = R + 2;
   extern __shared__ __align__(16) double smyz[];
   double* const stab = smyz;
@@ -974,57 +974,113 @@ __global__ void __launch_bounds__(32 * YZ_NL, ACC ? 3 : 4) kf_yt(const __grid_co
   cp_async_wait<0>();
 }
 
-// The lines of direction D that cross the interface, one warp per line:
+// The lines of direction D that cross the interface, in tiles of CW entries
+// of their list (which is in memory order, so a tile's lines are mostly
+// neighbours): the rows are copied in with cp.async, the next tile's while
+// this one is solved, and warp w solves entry w with its own coefficients
+// (loaded while the copy lands) and its blocks' Convert2Tri row operations.
 // y in place on d*, z (ACC) with the update of u.
+template <int MX, bool ACC>
+__host__ __device__ constexpr size_t yc_smem() {
+  // two buffers of CW lines x (R + 2), the lines' q (CW x R), ACC: u^n
+  return sizeof(double) * ((size_t)(ACC ? 3 : 2) * CW * (32 * MX + 2) + (size_t)CW * 32 * MX);
+}
+
 template <int D, int MX, bool ACC>
 __global__ void __launch_bounds__(32 * CW, 3) kf_yc(const __grid_constant__ Dev P, double* __restrict__ f,
                                                     double* __restrict__ u) {
   static_assert(D == 1 || D == 2, "y and z lines");
   constexpr int R = 32 * MX;
+  constexpr int LS = R + 2;
   extern __shared__ __align__(16) double smc[];
+  double* const bufs = smc;                      // [2][CW][LS]
+  double* const qbufs = smc + 2 * CW * LS;       // [CW][R]
+  double* const ubuf = qbufs + CW * R;           // [CW][LS] (ACC)
   const int nx = P.nx;
   const int n = D == 1 ? P.ny : P.nz;
   const int n2 = D == 1 ? P.nz : P.ny;
   const long long s = D == 1 ? (long long)nx : (long long)nx * P.ny;
   const long long s2 = D == 1 ? (long long)nx * P.ny : (long long)nx;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* const buf = smc + 2 * w * R;
-  double* const qbuf = buf + R;
-  const int jb = lane * MX;
+  const int c = threadIdx.x % CW, jc = threadIdx.x / CW;  // copy share: entry c, rows jc + 32 m
   const int nc = P.nfcross[D];
-  for (int c = blockIdx.x * CW + w; c < nc; c += gridDim.x * CW) {
-    const long long lid = P.fcross[D][c];
-    const long long base = lid / n2 + s2 * (lid % n2);
-    const int bfirst = P.bstart[D][lid], bend = P.bstart[D][lid + 1];
+  const int ntile = (nc + CW - 1) / CW;
+  const int32_t* const list = P.fcross[D];
+  // the rows past the line end stay 0 (the copies never write them)
+  for (int i = threadIdx.x; i < 2 * CW * LS; i += blockDim.x) bufs[i] = 0.0;
+  __syncthreads();
+  auto base_of = [&](long long lid) { return lid / n2 + s2 * (lid % n2); };
+  // entry i of tile t: its line (-1: none)
+  auto lid_of = [&](int t, int i) -> long long {
+    const int e = t * CW + i;
+    return (t < ntile && e < nc) ? (long long)list[e] : -1;
+  };
+  auto copy_rows = [&](long long lid, const double* src, double* cb) {
+    if (lid >= 0) {
+      const long long g0 = base_of(lid) + (long long)jc * s;
+#pragma unroll
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) cp_async8(cb + j, src + g0 + (long long)32 * m * s);
+      }
+    }
+    cp_async_commit();
+  };
+
+  int t = blockIdx.x;
+  long long lc0 = lid_of(t, c), lc1 = lid_of(t + gridDim.x, c);  // this thread's copy entry, two tiles
+  long long lw0 = lid_of(t, w), lw1 = lid_of(t + gridDim.x, w);  // this warp's solve entry
+  copy_rows(lc0, f, bufs + c * LS);
+  for (int it = 0; t < ntile; it++) {
+    const long long lc2 = lid_of(t + 2 * gridDim.x, c), lw2 = lid_of(t + 2 * gridDim.x, w);
+    double* const buf = bufs + (size_t)(it & 1) * CW * LS;
+    if (ACC) copy_rows(lc0, u, ubuf + c * LS);
+    copy_rows(lc1, f, bufs + (size_t)((it + 1) & 1) * CW * LS + c * LS);
+    // this warp's line: its coefficients and blocks, read while the rows land
     LineCoef<MX> cf;
-    cf.load(P.fcoef[D] + (size_t)c * 2 * R, lane);
-    double uv[MX];
+    int bfirst = 0, bend = 0;
+    if (lw0 >= 0) {
+      cf.load(P.fcoef[D] + (size_t)(t * CW + w) * 2 * R, lane);
+      bfirst = P.bstart[D][lw0];
+      bend = P.bstart[D][lw0 + 1];
+    }
+    if (ACC)
+      cp_async_wait<2>();
+    else
+      cp_async_wait<1>();
+    __syncthreads();
+    if (lw0 >= 0) {
+      double* const lb = buf + w * LS;
+      double* const qb = qbufs + w * R;
+      cf.put_q(qb, lane);
+      __syncwarp();
+      block_rows<D>(P, lb, qb, bfirst, bend, lane, true);
+      __syncwarp();
+      solve_cross<MX>(lb, qb, cf, n, lane);
+    }
+    if (ACC) cp_async_wait<1>();
+    __syncthreads();
+    if (lc0 >= 0) {
+      const long long g0 = base_of(lc0) + (long long)jc * s;
+      const double* const cb = buf + c * LS;
 #pragma unroll
-    for (int k = 0; k < MX; k++) {
-      const int j = jb + k;
-      if (j < n) {
-        buf[j] = f[base + (long long)j * s];
-        if (ACC) uv[k] = u[base + (long long)j * s];
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) {
+          if (ACC)
+            u[g0 + (long long)32 * m * s] = ubuf[c * LS + j] + cb[j];
+          else
+            f[g0 + (long long)32 * m * s] = cb[j];
+        }
       }
     }
-    cf.put_q(qbuf, lane);
-    __syncwarp();
-    block_rows<D>(P, buf, qbuf, bfirst, bend, lane, true);
-    __syncwarp();
-    solve_cross<MX>(buf, qbuf, cf, n, lane);
-    // (each lane reads back the rows it wrote)
-#pragma unroll
-    for (int k = 0; k < MX; k++) {
-      const int j = jb + k;
-      if (j < n) {
-        if (ACC)
-          u[base + (long long)j * s] = uv[k] + buf[j];
-        else
-          f[base + (long long)j * s] = buf[j];
-      }
-    }
-    __syncwarp();
+    t += gridDim.x;
+    lc0 = lc1;
+    lc1 = lc2;
+    lw0 = lw1;
+    lw1 = lw2;
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -1250,8 +1306,8 @@ void launch_yt(const Dev& P, double* f, double* u, cudaStream_t st) {
 }
 template <int D, int MX, bool ACC>
 void launch_yc(const Dev& P, double* f, double* u, cudaStream_t st) {
-  const int grid = resident_grid(P, kf_yc<D, MX, ACC>, 32 * CW, cross_smem<MX>(), (P.nfcross[D] + CW - 1) / CW);
-  kf_yc<D, MX, ACC><<<grid, 32 * CW, cross_smem<MX>(), st>>>(P, f, u);
+  const int grid = resident_grid(P, kf_yc<D, MX, ACC>, 32 * CW, yc_smem<MX, ACC>(), (P.nfcross[D] + CW - 1) / CW);
+  kf_yc<D, MX, ACC><<<grid, 32 * CW, yc_smem<MX, ACC>(), st>>>(P, f, u);
 }
 
 #define MTS_FAST_MX(X) X(1) X(3) X(5) X(9) X(13) X(17)
@@ -1284,8 +1340,8 @@ void fast_attr() {
   cudaFuncSetAttribute(kf_yt<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)yt_smem<MX, false>());
   cudaFuncSetAttribute(kf_yt<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yt_smem<MX, true>());
-  cudaFuncSetAttribute(kf_yc<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
-  cudaFuncSetAttribute(kf_yc<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
+  cudaFuncSetAttribute(kf_yc<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yc_smem<MX, false>());
+  cudaFuncSetAttribute(kf_yc<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yc_smem<MX, true>());
 }
 
 }  // namespace
