@@ -28,12 +28,12 @@
 //   kf_xc   the same for the x lines that cross the interface (side stream);
 //   kf_yt   the regular y lines, solved in place on d*, in tiles of NL
 //           neighbouring lines (the same row of NL lines is NL consecutive
-//           doubles) copied into shared memory by 16-byte cp.async chunks,
-//           double-buffered so that the next tile's copy overlaps this
-//           tile's solves;
+//           doubles) copied into shared memory with cp.async, double-buffered
+//           so that the next tile's copy overlaps this tile's solves;
 //   kf_yc   the y lines that cross the interface, one warp per line, their
 //           Convert2Tri row operations first (side stream);
-//   kf_yt / kf_yc for z, with the update u^{n+1} = u^n + d.
+//   kf_yt / kf_yc for z, with the update u^{n+1} = u^n + d (u^n of a tile
+//           is copied in while the tile is solved).
 //
 // Line solve: with the Thomas factors fixed (bet_j, gam_j of TDMA,
 // douglas_adi.cc:1784-1807), both recurrences are first-order and linear:
@@ -851,56 +851,45 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_xc(const __grid_constant__ Dev 
 // ---------------------------------------------------------------------------
 // The y and z passes.
 
-// Tiles of kf_yt are row-major in shared memory: row j of the tile's NL
-// lines is copied as 16-byte chunks from the 16-byte boundary at or below its
-// first element, into a row of YT_RS doubles; element (line c, row j) sits at
-// j YT_RS + sh(j) + c, sh(j) being the parity of the row's first element.
-// With YT_RS = 18, a lane's rows l MX + k (MX odd) fall on at most two lanes
-// per bank pair.
-constexpr int YT_RS = 18;
-constexpr int YT_CH = 9;  // 16-byte chunks per row (NL + 1 doubles, rounded up)
-static_assert(YZ_NL == 16, "the chunk layout is written for 16 lines");
-
-template <int MX>
+template <int MX, bool ACC>
 __host__ __device__ constexpr size_t yt_smem() {
-  // row tables 2 TABW; two row-major buffers of R rows x YT_RS doubles
-  return sizeof(double) * ((size_t)2 * tabw<MX>() + (size_t)2 * 32 * MX * YT_RS);
-}
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+  // row tables 2 TABW; two buffers of NL lines x (R + 2) doubles; ACC: one
+  // buffer of u^n
+  return sizeof(double) * ((size_t)2 * tabw<MX>() + (size_t)(ACC ? 3 : 2) * YZ_NL * (32 * MX + 2));
 }
 
 // The regular lines of direction D in tiles: y in place on d*; z (ACC) with
 // the update of u, face lines included (their d** passes through).
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * YZ_NL, 2) kf_yt(const __grid_constant__ Dev P, double* __restrict__ f,
-                                                       double* __restrict__ u, int ntiles) {
+__global__ void __launch_bounds__(32 * YZ_NL, ACC ? 1 : 2) kf_yt(const __grid_constant__ Dev P,
+                                                                  double* __restrict__ f, double* __restrict__ u,
+                                                                  int ntiles) {
   static_assert(D == 1 || D == 2, "y and z lines");
   constexpr int R = 32 * MX;
-  constexpr int TB = R * YT_RS;  // doubles per tile buffer
+  // line stride 2 mod 16 doubles: a lane's stride-MX rows (MX odd) fall on
+  // distinct bank pairs
+  constexpr int LS = R + 2;
   extern __shared__ __align__(16) double smyz[];
   double* const stab = smyz;
   double* const bufs = smyz + 2 * tabw<MX>();
+  double* const ubuf = bufs + 2 * YZ_NL * LS;  // (ACC)
   const int nx = P.nx;
   const int n = D == 1 ? P.ny : P.nz;
   const int n2 = D == 1 ? P.nz : P.ny;  // the second line index: iz (y lines) or iy (z lines)
   const long long s = D == 1 ? (long long)nx : (long long)nx * P.ny;   // row stride
   const long long s2 = D == 1 ? (long long)nx * P.ny : (long long)nx;  // stride of the second line index
-  const int sp = (int)(s & 1);
   // y tiles cover the interior lines (face y lines keep d*); z tiles cover
   // every line (face z lines pass d** through to the update)
   const int i1lo = ACC ? 0 : 1, i1n = ACC ? nx : nx - 2;
   const int i2lo = ACC ? 0 : 1;
   const int tpr = (i1n + YZ_NL - 1) / YZ_NL;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = threadIdx.x % YZ_NL, jc = threadIdx.x / YZ_NL;  // this thread's copy share: line c, rows jc + 32 m
   const uint8_t* const fline = P.fline[D];
-  const int nchunk = n * YT_CH;
 
   load_tab(stab, P.ftab[D], 2 * tabw<MX>());
   // the rows past the line end stay 0 (the copies never write them)
-  for (int i = threadIdx.x; i < 2 * TB; i += blockDim.x) bufs[i] = 0.0;
+  for (int i = threadIdx.x; i < 2 * YZ_NL * LS; i += blockDim.x) bufs[i] = 0.0;
   __syncthreads();
 
   struct Tile {
@@ -914,21 +903,21 @@ __global__ void __launch_bounds__(32 * YZ_NL, 2) kf_yt(const __grid_constant__ D
     T.ok = t < ntiles;
     return T;
   };
-  // flags of line `lane` (< NL) of tile T, -1: no line there; bit0 crosses
-  // the interface (left to kf_yc), bit1 side of row 1
-  auto flags = [&](const Tile& T) -> int {
-    const int i1 = T.i1 + lane;
-    if (!T.ok || lane >= YZ_NL || i1 >= i1lo + i1n) return -1;
+  // flags of line i of tile T (-1: no line there); bit0 crosses the
+  // interface (left to kf_yc), bit1 side of row 1
+  auto flags = [&](const Tile& T, int i) -> int {
+    const int i1 = T.i1 + i;
+    if (!T.ok || i1 >= i1lo + i1n) return -1;
     return fline[(long long)i1 * n2 + T.i2];
   };
-  auto first = [&](const Tile& T) { return T.i1 + s2 * T.i2; };  // row 0 of line 0
-  auto copy_in = [&](const Tile& T, double* buf) {
-    if (T.ok) {
-      const long long g0 = first(T);
-      for (int i = threadIdx.x; i < nchunk; i += blockDim.x) {
-        const int j = i / YT_CH, q = i - YT_CH * j;
-        const long long g = g0 + (long long)j * s;
-        cp_async16(buf + j * YT_RS + 2 * q, f + (g & ~1LL) + 2 * q);
+  auto copy_rows = [&](const Tile& T, int fc, const double* src, double* buf) {
+    if (fc >= 0 && !(fc & 1)) {
+      const long long g0 = T.i1 + c + s2 * T.i2 + (long long)jc * s;
+      double* const cb = buf + c * LS;
+#pragma unroll
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) cp_async8(cb + j, src + g0 + (long long)32 * m * s);
       }
     }
     cp_async_commit();
@@ -937,76 +926,50 @@ __global__ void __launch_bounds__(32 * YZ_NL, 2) kf_yt(const __grid_constant__ D
   int t = blockIdx.x;
   Tile cur = tile_of(t);
   Tile nxt = tile_of(t + gridDim.x);
-  // line flags, two tiles ahead (lane i < NL holds line i's)
-  int fl0 = flags(cur), fl1 = flags(nxt);
-  copy_in(cur, bufs);
+  // flags are read two tiles ahead: this thread's copy line (fc*) and this
+  // warp's solve line (fw*)
+  int fc0 = flags(cur, c), fc1 = flags(nxt, c);
+  int fw0 = flags(cur, w), fw1 = flags(nxt, w);
+  copy_rows(cur, fc0, f, bufs);
   for (int it = 0; cur.ok; it++) {
     const Tile nx2 = tile_of(t + 2 * gridDim.x);
-    const int fl2 = flags(nx2);
-    double* const buf = bufs + (size_t)(it & 1) * TB;
-    copy_in(nxt, bufs + (size_t)((it + 1) & 1) * TB);
-    // the lines this tile stores: present and not crossing the interface
-    const unsigned keep = __ballot_sync(FULL, fl0 >= 0 && !(fl0 & 1)) & 0xffffu;
-    const int fw = __shfl_sync(FULL, fl0, w);
-    cp_async_wait<1>();
+    const int fc2 = flags(nx2, c), fw2 = flags(nx2, w);
+    double* const buf = bufs + (size_t)(it & 1) * YZ_NL * LS;
+    if (ACC) copy_rows(cur, fc0, u, ubuf);
+    copy_rows(nxt, fc1, f, bufs + (size_t)((it + 1) & 1) * YZ_NL * LS);
+    if (ACC)
+      cp_async_wait<2>();
+    else
+      cp_async_wait<1>();
     __syncthreads();
-    const long long g0 = first(cur);
-    const int sh0 = (int)(g0 & 1);
     {
       const int i1 = cur.i1 + w;
       const bool interior = i1 >= 1 && i1 <= nx - 2 && cur.i2 >= 1 && cur.i2 <= n2 - 2;
-      if (((keep >> w) & 1) && interior) {
-        const int jb = lane * MX;
-        double y[MX];
-#pragma unroll
-        for (int k = 0; k < MX; k++) {
-          const int j = jb + k;
-          y[k] = buf[j * YT_RS + (sh0 ^ (j & sp)) + w];
-        }
-        solve_lean<MX>(y, stab + ((fw >> 1) & 1) * tabw<MX>(), lane);
-#pragma unroll
-        for (int k = 0; k < MX; k++) {
-          const int j = jb + k;
-          buf[j * YT_RS + (sh0 ^ (j & sp)) + w] = y[k];
-        }
-      }
+      if (fw0 >= 0 && !(fw0 & 1) && interior) solve_tab<MX>(buf + w * LS, stab + ((fw0 >> 1) & 1) * tabw<MX>(), lane);
     }
+    if (ACC) cp_async_wait<1>();
     __syncthreads();
-    // out by 16-byte chunks where both of a chunk's lines are stored, 8 bytes
-    // at the edges of the tile and beside lines that are not
-    for (int i = threadIdx.x; i < nchunk; i += blockDim.x) {
-      const int j = i / YT_CH, q = i - YT_CH * j;
-      const long long g = g0 + (long long)j * s;
-      const int lo = 2 * q - (int)(g & 1);
-      const bool okl = lo >= 0 && ((keep >> lo) & 1);
-      const bool okh = lo + 1 < YZ_NL && ((keep >> (lo + 1)) & 1);
-      if (!okl && !okh) continue;
-      const double* const v = buf + j * YT_RS + 2 * q;
-      double* const o = (ACC ? u : f) + (g & ~1LL) + 2 * q;
-      double2 x = make_double2(v[0], v[1]);
-      if (ACC) {
-        if (okl && okh) {
-          const double2 a = *reinterpret_cast<const double2*>(o);
-          x.x += a.x;
-          x.y += a.y;
-        } else if (okl) {
-          x.x += o[0];
-        } else {
-          x.y += o[1];
+    if (fc0 >= 0 && !(fc0 & 1)) {
+      const long long g0 = cur.i1 + c + s2 * cur.i2 + (long long)jc * s;
+      const double* const cb = buf + c * LS;
+#pragma unroll
+      for (int m = 0; m < MX; m++) {
+        const int j = jc + 32 * m;
+        if (j < n) {
+          if (ACC)
+            u[g0 + (long long)32 * m * s] = ubuf[c * LS + j] + cb[j];
+          else
+            f[g0 + (long long)32 * m * s] = cb[j];
         }
       }
-      if (okl && okh)
-        *reinterpret_cast<double2*>(o) = x;
-      else if (okl)
-        o[0] = x.x;
-      else
-        o[1] = x.y;
     }
     t += gridDim.x;
     cur = nxt;
     nxt = nx2;
-    fl0 = fl1;
-    fl1 = fl2;
+    fc0 = fc1;
+    fc1 = fc2;
+    fw0 = fw1;
+    fw1 = fw2;
   }
   cp_async_wait<0>();
 }
@@ -1338,8 +1301,8 @@ void launch_yt(const Dev& P, double* f, double* u, cudaStream_t st) {
   const int n2 = D == 1 ? P.nz : P.ny;
   const int rows = ACC ? n2 : n2 - 2;
   const int ntiles = (i1n + YZ_NL - 1) / YZ_NL * rows;
-  const int grid = resident_grid(P, kf_yt<D, MX, ACC>, 32 * YZ_NL, yt_smem<MX>(), ntiles);
-  kf_yt<D, MX, ACC><<<grid, 32 * YZ_NL, yt_smem<MX>(), st>>>(P, f, u, ntiles);
+  const int grid = resident_grid(P, kf_yt<D, MX, ACC>, 32 * YZ_NL, yt_smem<MX, ACC>(), ntiles);
+  kf_yt<D, MX, ACC><<<grid, 32 * YZ_NL, yt_smem<MX, ACC>(), st>>>(P, f, u, ntiles);
 }
 template <int D, int MX, bool ACC>
 void launch_yc(const Dev& P, double* f, double* u, cudaStream_t st) {
@@ -1374,8 +1337,9 @@ void fast_attr() {
   cudaFuncSetAttribute(kf_xw<8, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSweepSmem);
   cudaFuncSetAttribute(kf_xw<4, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSweepSmem);
   cudaFuncSetAttribute(kf_xc<MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cross_smem<MX>());
-  cudaFuncSetAttribute(kf_yt<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yt_smem<MX>());
-  cudaFuncSetAttribute(kf_yt<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yt_smem<MX>());
+  cudaFuncSetAttribute(kf_yt<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yt_smem<MX, false>());
+  cudaFuncSetAttribute(kf_yt<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yt_smem<MX, true>());
   cudaFuncSetAttribute(kf_yc<1, MX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yc_smem<MX, false>());
   cudaFuncSetAttribute(kf_yc<2, MX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yc_smem<MX, true>());
 }
