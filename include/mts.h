@@ -153,7 +153,8 @@ mts_status mts_advance_host(mts_handle h, const double* u_in, double* u_out, int
 
 /* Error (douglas_adi.cc:1723-1770): L-infinity with its first argmax in
  * [ix][iy][iz] loop order, and L2 = sqrt(sum e^2 / (nx ny nz)), against the
- * exact solution at the current time.  Synchronous. */
+ * exact solution at the current time.  Synchronous; on an error status the
+ * outputs are left untouched. */
 mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3);
 
 /* The same norms with no allocation of any kind.  This entry point has no
@@ -172,9 +173,11 @@ mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3);
  * 4194304 nodes (2048 x 2048) are rejected with MTS_ERR_ARG.  Its ticket
  * counter must be zero when the kernel starts; each call clears it first.
  * All calls on a device share the array, so calls that overlap in time on one
- * device (other handles, streams or host threads) race: serialise them.  The
- * first call on a device looks the array's address up (and may load the
- * module); make that call before any stream capture begins on the device. */
+ * device (other handles, streams or host threads) race: serialise them.  Each
+ * call looks the array's address up again, so a device reset between calls
+ * is harmless; the first call on a device may load the module, so make it
+ * before any stream capture begins on the device.  On an error status the
+ * outputs are left untouched. */
 mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double* lmax, double* l2,
                              int32_t* argmax3);
 

@@ -9,7 +9,6 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -979,9 +978,10 @@ mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3) {
   if (!h) return fail(MTS_ERR_ARG, "null handle");
   h->launches += mts::launch_norms(h->dev, std::exp(-h->t), h->u0, h->norm_part, h->norm_nb, h->norm_out, h->stream);
   CUDA_TRY(cudaGetLastError());
-  double r[3];
+  double r[3] = {0.0, 0.0, 0.0};
   CUDA_TRY(cudaMemcpyAsync(r, h->norm_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   mts_status st = sync_status(h);
+  if (st != MTS_OK) return st;
   if (lmax) *lmax = r[0];
   if (l2) *l2 = r[2];
   if (argmax3) {
@@ -1013,25 +1013,18 @@ mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double
                                  std::to_string(nb) + " reduction blocks; the static scratch holds " +
                                  std::to_string(mts::kNoAllocMaxBlocks) + " (grids of at most " +
                                  std::to_string((long long)mts::kNoAllocMaxBlocks * 2048) + " nodes)");
-  constexpr int kMaxDevices = 64;
-  if (h->device < 0 || h->device >= kMaxDevices) return fail(MTS_ERR_ARG, "device ordinal out of range");
-  static std::mutex lock;
-  static double* addr[kMaxDevices] = {};
+  // The scratch's address is looked up on every call (cheap once the module
+  // is loaded), so a device reset or a new primary context between calls
+  // never leaves a stale address behind.
   double* scratch = nullptr;
   {
-    std::lock_guard<std::mutex> g(lock);
-    if (!addr[h->device]) {
-      int cur = -1;
-      CUDA_TRY(cudaGetDevice(&cur));
-      if (cur != h->device) CUDA_TRY(cudaSetDevice(h->device));
-      double* p = nullptr;
-      cudaError_t e = mts::noalloc_scratch_address(&p);
-      if (cur != h->device) cudaSetDevice(cur);
-      if (e != cudaSuccess)
-        return fail(MTS_ERR_CUDA, std::string("cudaGetSymbolAddress(static norms scratch): ") + cudaGetErrorString(e));
-      addr[h->device] = p;
-    }
-    scratch = addr[h->device];
+    int cur = -1;
+    CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != h->device) CUDA_TRY(cudaSetDevice(h->device));
+    cudaError_t e = mts::noalloc_scratch_address(&scratch);
+    if (cur != h->device) cudaSetDevice(cur);
+    if (e != cudaSuccess)
+      return fail(MTS_ERR_CUDA, std::string("cudaGetSymbolAddress(static norms scratch): ") + cudaGetErrorString(e));
   }
   const double* u = u_dev ? u_dev : h->u0;
   const double tt = u_dev ? t : h->t;
@@ -1039,9 +1032,10 @@ mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double
   CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned), h->stream));
   h->launches += mts::launch_norms_noalloc(h->dev, std::exp(-tt), u, scratch, nb, h->stream);
   CUDA_TRY(cudaGetLastError());
-  double r[3];
+  double r[3] = {0.0, 0.0, 0.0};
   CUDA_TRY(cudaMemcpyAsync(r, scratch + 32, sizeof r, cudaMemcpyDeviceToHost, h->stream));
   mts_status st = sync_status(h);
+  if (st != MTS_OK) return st;
   if (lmax) *lmax = r[0];
   if (l2) *l2 = r[2];
   if (argmax3) {

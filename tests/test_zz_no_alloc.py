@@ -60,3 +60,26 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
         with pytest.raises(RuntimeError, match="static scratch holds 2048"):
             s.norms_noalloc()
         assert s.norms() == ref
+
+
+def test_noalloc_two_handles_in_turn():
+    """Two handles on one device, each with its own stream, call the entry
+    point one after the other (serialised, as the shared scratch requires);
+    each result equals that handle's own mts_norms."""
+    with M.Solver(spec(65, "torus", "adi")) as a, M.Solver(spec(49, "ellipsoid", "ts")) as b:
+        assert a.stream() != b.stream()
+        for s in (a, b):
+            s.initialize()
+            s.advance(2)
+            s.synchronize()
+        refs = {id(a): a.norms(), id(b): b.norms()}
+        assert refs[id(a)] != refs[id(b)]
+        for _ in range(3):
+            for s in (a, b, b, a):
+                assert s.norms_noalloc() == refs[id(s)]
+        a.advance(1)
+        b.advance(1)
+        a.synchronize()
+        b.synchronize()
+        ra, rb = a.norms(), b.norms()
+        assert a.norms_noalloc() == ra and b.norms_noalloc() == rb
