@@ -208,3 +208,29 @@ def test_fast_on_a_problem_sensitive_to_rounding():
     u_p, _, _ = run(spec, 4, "plain")
     u_f, _, _ = run(spec, 4, "fast")
     assert rel_maxdiff(u_f, u_p) <= 1e-4
+
+
+@pytest.mark.parametrize("mib", [1, 2])
+@pytest.mark.parametrize("surface,params", [("ellipsoid", SPHERE), ("ellipsoid", ELLIPSOID), ("torus", TORUS)],
+                         ids=["sphere", "ellipsoid", "torus"])
+def test_fast_matches_oracle_129(surface, params, mib):
+    """129^3 (beta 1:1000, dt = h), 2 steps, every interface and MIB variant."""
+    spec = M.Spec(n=(129, 129, 129), surface=surface, surface_params=params, beta_in=1.0, beta_out=1000.0,
+                  method="adi", mib=mib, dt=2.0 / 128)
+    tags, cr, _ = M.setup_host(spec)
+    prob = O.Problem(n=(129, 129, 129), surface=surface, surface_params=params, beta_in=1.0, beta_out=1000.0,
+                     method="adi", mib=mib, dt=2.0 / 128, steps=2)
+    u_or = O.port_run(prob, tags, cr, O.port_init(prob, tags))
+    u, (lmax, l2, _), t = run(spec, 2)
+    assert rel_maxdiff(u, u_or) <= TOL
+    lo, l2o, _ = O.port_norms(prob, tags, t, u_or)
+    assert close_norms(lmax, lo) and close_norms(l2, l2o)
+
+
+@pytest.mark.parametrize("params", [SPHERE, ELLIPSOID], ids=["sphere", "ellipsoid"])
+def test_fast_257_l1(params):
+    spec = M.Spec(n=(257, 257, 257), surface="ellipsoid", surface_params=params, beta_in=1.0, beta_out=1000.0,
+                  method="adi", mib=1, dt=2.0 / 256)
+    u_p, _, _ = run(spec, 2, "plain")
+    u_f, _, _ = run(spec, 2, "fast")
+    assert rel_maxdiff(u_f, u_p) <= TOL
