@@ -581,9 +581,11 @@ def main():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push(f"timed_steps_{precision}")
         m0.record(st_)
         sv.advance(a.steps)
         m1.record(st_)
+        torch.cuda.nvtx.range_pop()
         sv.synchronize()
         ms_ = m0.elapsed_time(m1)
         km, kc = sv.profile_read()
