@@ -20,6 +20,7 @@ Prints one JSON line (rank 0).
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -100,10 +101,8 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served-form run")
     ap.add_argument("--batch-problems", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=50)
-    ap.add_argument("--served-requests", type=int, default=3000,
-                    help="requests per arrival rate (3000: the 1000 req/s stream reaches its steady state; "
-                         "the full served workload is 10000)")
-    ap.add_argument("--served-rates", default="200,1000", help="Poisson arrival rates, requests/s")
+    ap.add_argument("--served-requests", type=int, default=10000, help="requests per arrival rate")
+    ap.add_argument("--served-rates", default="1000,2000", help="Poisson arrival rates, requests/s")
     ap.add_argument("--workload", default="step", choices=["step", "precision", "batched", "served"],
                     help="step: the headline line (default); precision / batched / served: the full sweep of "
                          "that form alone, one JSON line")
@@ -176,8 +175,15 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
     import mts_b200 as M
     from mts_b200.workloads import batched_problems
 
-    t_setup = time.perf_counter()
     specs = batched_problems(count, seed)
+    # the host setup alone (tags, crossings, MIB weights on host threads), for
+    # comparison with the device setup the run uses
+    t_host = time.perf_counter()
+    for sp in specs:
+        M.setup_host(sp)
+    t_host = time.perf_counter() - t_host
+    specs = [dataclasses.replace(sp, setup="device") for sp in specs]
+    t_setup = time.perf_counter()
     solvers = [M.Solver(sp) for sp in specs]
     t_setup = time.perf_counter() - t_setup
     nodes = sum(sp.n[0] * sp.n[1] * sp.n[2] for sp in specs)
@@ -211,7 +217,10 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
         "problems": count, "steps": steps, "seed": seed, "nodes_total": nodes,
         "sequential_solves_per_s": count / seq, "batched_solves_per_s": count / bat,
         "speedup": seq / bat, "batched_cell_steps_per_s": nodes * steps / bat,
-        "sequential_s": seq, "batched_s": bat, "host_setup_s": t_setup, "results_identical": same,
+        "sequential_s": seq, "batched_s": bat, "create_s": t_setup, "host_setup_only_s": t_host,
+        "setup": "device (mts_create with setup = device: tags, crossing scan, rtsafe and MIB weight LU on the GPU; "
+                 "create_s also holds the upload of every problem)",
+        "results_identical": same,
         "timing": "wall clock between synchronizations (launch and graph overheads included)",
         "family": "grids U{17,25,33,49,65}^3, shifted ellipsoids, beta_out log-uniform [1e-3,1e3], "
                   "methods U{ADI,LOD-IE,LOD-CN,TS} x MIB-L1/L2, dt = min h, plain FP64, numpy PCG64 seed 0",
@@ -220,35 +229,57 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
 
 def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 120e9) -> dict:
     """Poisson streams of `count` requests per rate through the continuous-
-    batching server, against the sequential plain solver on the same stream
-    (its service times measured on a sample, its queue modelled FIFO)."""
+    batching server, against the sequential plain solver on the same stream.
+    Both use the device setup.  The sequential service time is measured on a
+    stratified sample of the stream (by grid class: the batched family's
+    grids, 129^3, 257^3), weighted by each class's share of the stream; its
+    latencies come from one FIFO solver fed the stream's arrivals with
+    service times drawn from the measured ones of each request's class."""
     import numpy as np
 
-    from mts_b200 import serve
-    from mts_b200.workloads import served_requests
+    from mts_b200 import serve, setup_device
+    from mts_b200.workloads import served_requests, size_class
 
-    out = {"requests_per_rate": count, "hbm_budget_bytes": budget, "rates": {}}
-    # sequential service time per request (setup, upload, steps, norms), on a
-    # sample of the stream, one request after another
-    sample = served_requests(min(count, 120), 1000.0, seed + 1)
-    svc = []
-    for q in sample:
-        t0 = time.perf_counter()
-        serve.solve_alone(q)
-        svc.append(time.perf_counter() - t0)
-    svc = np.array(svc)
-    out["sequential_solves_per_s"] = float(1.0 / svc.mean())
-    out["sequential_service_sample"] = len(svc)
+    def on_device(reqs):
+        for q in reqs:
+            q.spec = dataclasses.replace(q.spec, setup="device")
+        return reqs
+
+    out = {"requests_per_rate": count, "hbm_budget_bytes": budget, "setup": "device", "rates": {}}
+    t_gen = time.perf_counter()
+    stream = on_device(served_requests(count, 1000.0, seed, validate=setup_device))
+    out["stream_generation_s"] = time.perf_counter() - t_gen
+    classes = {}
+    for q in stream:
+        classes.setdefault(size_class(q.spec), []).append(q)
+    share = {c: len(v) / len(stream) for c, v in classes.items()}
+    per_class = {"small": 48, "129": 16, "257": 6}
+    rs = np.random.default_rng(seed + 1)
+    svc = {}
+    serve.solve_alone(stream[0])  # module loading and first-launch costs, not timed
+    for c, v in classes.items():
+        pick = rs.choice(len(v), min(per_class.get(c, 8), len(v)), replace=False)
+        times = []
+        for i in pick:
+            t0 = time.perf_counter()
+            serve.solve_alone(v[int(i)])
+            times.append(time.perf_counter() - t0)
+        svc[c] = np.array(times)
+    mean_svc = sum(share[c] * svc[c].mean() for c in svc)
+    out["sequential_solves_per_s"] = float(1.0 / mean_svc)
+    out["sequential_sample"] = {c: {"share": share[c], "sampled": int(len(svc[c])), "mean_s": float(svc[c].mean())}
+                                for c in svc}
     rng = np.random.default_rng(seed + 2)
     for rate in rates:
-        reqs = served_requests(count, rate, seed)
-        srv = serve.Server(hbm_budget=budget)
+        reqs = on_device(served_requests(count, rate, seed, validate=setup_device))
+        srv = serve.Server(hbm_budget=budget, setup="device")
         t0 = time.perf_counter()
         res = srv.run(reqs)
         span = time.perf_counter() - t0
         lat = np.array([r.latency for r in res])
         arr = np.array([q.arrival for q in reqs])
-        seq_lat = serve.fifo_latencies(arr, rng.choice(svc, len(arr)))
+        seq_svc = np.array([rng.choice(svc[size_class(q.spec)]) for q in reqs])
+        seq_lat = serve.fifo_latencies(arr, seq_svc)
         out["rates"][str(rate)] = {
             "solves_per_s": len(res) / span, "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)), "sequential_p50_s": float(np.percentile(seq_lat, 50)),
@@ -258,7 +289,8 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
             "solves_per_s_vs_sequential": len(res) / span / out["sequential_solves_per_s"],
         }
     out["timing"] = ("wall clock from the first arrival to the last completion; latency = completion - arrival; "
-                     "the sequential latencies model one FIFO solver with the sampled service times")
+                     "sequential: service times measured per grid class on a stratified sample, latencies from a "
+                     "FIFO queue over the same arrivals")
     return out
 
 

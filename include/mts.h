@@ -53,17 +53,22 @@ typedef struct {
   double params[7];
 } mts_surface;
 
+/* Where mts_create builds the tags, crossings and MIB weights. */
+typedef enum { MTS_SETUP_HOST = 0, MTS_SETUP_DEVICE = 1 } mts_setup_where;
+
 /* Problem parameters.  beta is piecewise constant (beta_in inside, beta_out
  * outside).  eq selects the exact solution that supplies source, boundary and
  * jump data: 0 = the reference's Eq_0 (src/equation/eq_0.cc), 8 = inside
  * e^{-t} sin2x cos2y sin2z / outside e^{-t}(x^2+y^2+z^2).  mib is 1 (MIB-L1)
- * or 2 (MIB-L2) as in Intersections(..., mib_method, ...). */
+ * or 2 (MIB-L2) as in Intersections(..., mib_method, ...).  setup
+ * (mts_setup_where) selects the host threads (0, the default) or the device
+ * (1) for mts_create's setup; see mts_setup_device. */
 typedef struct {
   double beta_in, beta_out;
   int32_t eq;
   int32_t method; /* mts_method */
   int32_t mib;
-  int32_t pad;
+  int32_t setup;  /* mts_setup_where */
   double dt;
   double t0;
 } mts_params;
@@ -105,6 +110,18 @@ mts_status mts_destroy(mts_handle h);
 mts_status mts_setup_host(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
                           int8_t* tags, mts_crossing* out, int32_t capacity, int32_t* count,
                           int64_t counts[2]);
+
+/* The same setup on the current CUDA device, with the same arguments and
+ * results: a thread per node for the tags, a thread per grid line for the
+ * crossing scan, rtsafe and the MIB-L1/L2 weight solves, a thread per corner
+ * pair for the MIB-L2 36x36 systems.  The tags equal mts_setup_host's; the
+ * crossing records equal them bit for bit except where the reference's
+ * pow(v, 2) (glibc) is not the correctly rounded square, which the device
+ * computes: there a root, normal or weight can differ in its last bits.
+ * Synchronous.  No reference counterpart beyond mts_setup_host's. */
+mts_status mts_setup_device(const mts_grid* grid, const mts_surface* surface, const mts_params* params,
+                            int8_t* tags, mts_crossing* out, int32_t capacity, int32_t* count,
+                            int64_t counts[2]);
 
 /* Initialization (douglas_adi.cc:1684-1714, lod/trapezoidal copies): the
  * exact solution at the current time, by node tag, written on the device. */

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/mts.h"
@@ -59,6 +60,15 @@ struct SetupReport {
 mts_status build_crossings(const Grid& g, const std::vector<int8_t>& tags, const Surface& s,
                            double beta_in, double beta_out, int mib,
                            std::vector<mts_crossing>& out, SetupReport* report);
+
+// build_tags + build_crossings on the current CUDA device (setup_gpu.cu),
+// queued on `stream` (a cudaStream_t) and synchronized before returning: the
+// same tags and crossing list, bit for bit except where the reference's
+// pow(v, 2) is not the correctly rounded square.  On failure `why` (may be
+// null) receives the reason.
+mts_status setup_on_device(const Grid& g, const mts_surface& surf, double beta_in, double beta_out, int mib,
+                           void* stream, std::vector<int8_t>& tags, std::vector<mts_crossing>& out,
+                           SetupReport* report, std::string* why);
 
 // (P^{-1})[row][0] of the 3x3 local frame via the reference LU inverse
 // (src/decomposition/lu.cc:15-161); returns false on an all-zero row.

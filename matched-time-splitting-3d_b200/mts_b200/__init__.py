@@ -22,6 +22,7 @@ __all__ = [
     "Spec",
     "Solver",
     "setup_host",
+    "setup_device",
     "batch_advance",
     "batch_advance_steps",
     "MtsError",
@@ -48,6 +49,7 @@ class Spec:
     mib: int = 1
     dt: float = 1.0 / 32
     t0: float = 0.0
+    setup: str = "host"  # where mts_create builds tags, crossings and MIB weights: host or device
 
     @property
     def nodes(self) -> int:
@@ -55,24 +57,35 @@ class Spec:
 
     def c_structs(self):
         return (make_grid(self.n, self.domain), make_surface(self.surface, self.surface_params),
-                make_params(self.beta_in, self.beta_out, self.eq, self.method, self.mib, self.dt, self.t0))
+                make_params(self.beta_in, self.beta_out, self.eq, self.method, self.mib, self.dt, self.t0,
+                            self.setup))
+
+
+def _setup(spec: Spec, name: str):
+    L = load()
+    fn = getattr(L, name)
+    g, s, p = spec.c_structs()
+    count = ctypes.c_int32(0)
+    check(fn(ctypes.byref(g), ctypes.byref(s), ctypes.byref(p), None, None, 0, ctypes.byref(count), None), name)
+    tags = np.empty(spec.nodes, dtype=np.int8)
+    cr = np.zeros(count.value, dtype=CROSSING_DTYPE)
+    counts = np.zeros(2, dtype=np.int64)
+    check(fn(ctypes.byref(g), ctypes.byref(s), ctypes.byref(p), tags.ctypes.data, cr.ctypes.data if cr.size else None,
+             cr.size, ctypes.byref(count), counts.ctypes.data), name)
+    return tags, cr, {"corner_pairs": int(counts[0]), "singular_warnings": int(counts[1])}
 
 
 def setup_host(spec: Spec):
     """Host setup only: returns (tags int8[N], crossings CROSSING_DTYPE[n],
     {"corner_pairs", "singular_warnings"})."""
-    L = load()
-    g, s, p = spec.c_structs()
-    count = ctypes.c_int32(0)
-    check(L.mts_setup_host(ctypes.byref(g), ctypes.byref(s), ctypes.byref(p), None, None, 0, ctypes.byref(count),
-                           None), "mts_setup_host")
-    tags = np.empty(spec.nodes, dtype=np.int8)
-    cr = np.zeros(count.value, dtype=CROSSING_DTYPE)
-    counts = np.zeros(2, dtype=np.int64)
-    check(L.mts_setup_host(ctypes.byref(g), ctypes.byref(s), ctypes.byref(p), tags.ctypes.data,
-                           cr.ctypes.data if cr.size else None, cr.size, ctypes.byref(count), counts.ctypes.data),
-          "mts_setup_host")
-    return tags, cr, {"corner_pairs": int(counts[0]), "singular_warnings": int(counts[1])}
+    return _setup(spec, "mts_setup_host")
+
+
+def setup_device(spec: Spec):
+    """The same setup on the CUDA device (mts_setup_device), same results:
+    tags identical, crossing records identical except in the last bits where
+    the reference's pow(v, 2) is not the correctly rounded square."""
+    return _setup(spec, "mts_setup_device")
 
 
 def batch_advance(solvers, nsteps: int) -> None:

@@ -32,6 +32,7 @@ EXPORTS = [
     "mts_create",
     "mts_create_from_crossings",
     "mts_setup_host",
+    "mts_setup_device",
     "mts_destroy",
     "mts_initialize",
     "mts_set_solution",
@@ -96,7 +97,7 @@ class mts_params(ctypes.Structure):
         ("eq", ctypes.c_int32),
         ("method", ctypes.c_int32),
         ("mib", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("setup", ctypes.c_int32),
         ("dt", ctypes.c_double),
         ("t0", ctypes.c_double),
     ]
@@ -154,6 +155,8 @@ def load(build_if_missing: bool = True):
             "mts_create_from_crossings": [P(mts_grid), vp, vp, ctypes.c_int32, P(mts_params), P(H)],
             "mts_setup_host": [P(mts_grid), P(mts_surface), P(mts_params), vp, vp, ctypes.c_int32,
                                P(ctypes.c_int32), vp],
+            "mts_setup_device": [P(mts_grid), P(mts_surface), P(mts_params), vp, vp, ctypes.c_int32,
+                                 P(ctypes.c_int32), vp],
             "mts_destroy": [H],
             "mts_initialize": [H],
             "mts_set_solution": [H, vp],
@@ -216,6 +219,9 @@ def make_surface(kind: str, params) -> mts_surface:
     return s
 
 
-def make_params(beta_in, beta_out, eq, method, mib, dt, t0=0.0) -> mts_params:
+SETUPS = {"host": 0, "device": 1}
+
+
+def make_params(beta_in, beta_out, eq, method, mib, dt, t0=0.0, setup="host") -> mts_params:
     m = METHODS[method] if isinstance(method, str) else int(method)
-    return mts_params(float(beta_in), float(beta_out), int(eq), m, int(mib), 0, float(dt), float(t0))
+    return mts_params(float(beta_in), float(beta_out), int(eq), m, int(mib), SETUPS[setup], float(dt), float(t0))

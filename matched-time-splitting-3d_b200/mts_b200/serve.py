@@ -25,7 +25,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import Solver, batch_advance_steps, setup_host
+from . import Solver, batch_advance_steps, setup_device, setup_host
 from .workloads import Request, device_bytes_bound
 
 
@@ -68,16 +68,22 @@ class Server:
       hundred problems more of them in flight lower the throughput.
     chunk_steps: steps per batch call; new arrivals join at chunk boundaries.
     host_threads: pool for host setup and uploads.
-    keep_solutions: keep each result's final field (for tests)."""
+    keep_solutions: keep each result's final field (for tests).
+    setup: "host" (tags, crossings and MIB weights on the pool's host
+      threads) or "device" (the same on the GPU, mts_setup_device)."""
 
     def __init__(self, hbm_budget: float = 120e9, chunk_steps: int = 8, host_threads: int = 16,
-                 keep_solutions: bool = False, precision: str = "plain", max_active: int = 256):
+                 keep_solutions: bool = False, precision: str = "plain", max_active: int = 256,
+                 setup: str = "host"):
         self.budget = int(hbm_budget)
         self.max_active = max(1, int(max_active))
         self.chunk = max(1, int(chunk_steps))
         self.threads = max(1, int(host_threads))
         self.keep = keep_solutions
         self.precision = precision
+        if setup not in ("host", "device"):
+            raise ValueError("setup must be host or device")
+        self.setup = setup_device if setup == "device" else setup_host
         self.peak_bytes = 0
         self.peak_active = 0
         self.batches = 0
@@ -88,7 +94,7 @@ class Server:
 
     # -- pool tasks ----------------------------------------------------------
     def _setup(self, job: _Job) -> _Job:
-        tags, cr, _ = setup_host(job.req.spec)
+        tags, cr, _ = self.setup(job.req.spec)
         job.tags, job.crossings = tags, cr
         job.bound = device_bytes_bound(job.req.spec, len(cr), precision=self.precision)
         return job

@@ -24,8 +24,12 @@ METHODS = ("adi", "lod-ie", "lod-cn", "ts")
 BATCH_SIZES = (17, 25, 33, 49, 65)
 
 
-def draw_problem(rng: np.random.Generator, sizes=BATCH_SIZES, n=None) -> Spec:
-    """One problem of the batched family (n forces the grid)."""
+def draw_problem(rng: np.random.Generator, sizes=BATCH_SIZES, n=None, validate=None) -> Spec:
+    """One problem of the batched family (n forces the grid).  validate is
+    the setup that accepts or rejects a draw (setup_host by default;
+    setup_device accepts and rejects the same draws: the family's ellipsoid
+    level set has no pow(v, 2))."""
+    validate = validate or setup_host
     while True:
         grid = tuple(int(v) for v in rng.choice(sizes, 3)) if n is None else tuple(n)
         axes = rng.uniform(0.3, 0.7, 3)
@@ -34,7 +38,7 @@ def draw_problem(rng: np.random.Generator, sizes=BATCH_SIZES, n=None) -> Spec:
                     beta_in=1.0, beta_out=float(10.0 ** rng.uniform(-3.0, 3.0)), method=METHODS[int(rng.integers(4))],
                     mib=int(rng.integers(1, 3)), dt=min(2.0 / (k - 1) for k in grid))
         try:
-            setup_host(spec)
+            validate(spec)
             return spec
         except MtsError:
             continue  # interface through a grid node: the reference rejects it too
@@ -53,18 +57,38 @@ class Request:
     arrival: float  # seconds after the start of the stream
 
 
-def served_requests(count: int, rate: float, seed: int = 0) -> list[Request]:
-    """A Poisson stream of `count` requests at `rate` per second."""
-    rng = np.random.default_rng(seed)
+_STREAMS: dict = {}
+
+
+def served_requests(count: int, rate: float, seed: int = 0, validate=None) -> list[Request]:
+    """A Poisson stream of `count` requests at `rate` per second.  The
+    problems and step counts do not depend on the rate (the gaps are one
+    series of standard exponential draws scaled by 1/rate), so they are drawn
+    once per (count, seed) and kept."""
+    key = (count, seed)
+    if key not in _STREAMS:
+        rng = np.random.default_rng(seed)
+        draws = []
+        for _ in range(count):
+            e = float(rng.standard_exponential())
+            u = rng.uniform()
+            n = (257, 257, 257) if u < 0.01 else (129, 129, 129) if u < 0.06 else None
+            spec = draw_problem(rng, BATCH_SIZES, n, validate)
+            draws.append((e, spec, int(rng.integers(20, 201))))
+        _STREAMS[key] = draws
     t = 0.0
     out = []
-    for i in range(count):
-        t += float(rng.exponential(1.0 / rate))
-        u = rng.uniform()
-        n = (257, 257, 257) if u < 0.01 else (129, 129, 129) if u < 0.06 else None
-        spec = draw_problem(rng, BATCH_SIZES, n)
-        out.append(Request(i, spec, int(rng.integers(20, 201)), t))
+    scale = 1.0 / rate
+    for i, (e, spec, steps) in enumerate(_STREAMS[key]):
+        t += scale * e
+        out.append(Request(i, spec, steps, t))
     return out
+
+
+def size_class(spec: Spec) -> str:
+    """The served stream's strata: the batched family's grids, 129^3, 257^3."""
+    m = max(spec.n)
+    return "257" if m >= 257 else "129" if m >= 129 else "small"
 
 
 def device_bytes_bound(spec: Spec, ncrossings: int, sms: int = 148, precision: str = "plain") -> int:
