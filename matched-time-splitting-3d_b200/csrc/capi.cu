@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -39,13 +40,15 @@ mts_status fail(mts_status s, const std::string& msg) {
 // server that creates and destroys problems continuously then neither
 // synchronizes the device on every free nor returns memory to the driver in
 // between (the pool keeps what it has, see configure_pool).  A handle takes
-// its memory from the pool as a few slabs and hands out its buffers from
-// them: a pool that holds many freed blocks makes every cudaMallocAsync
-// slower (measured on B200: 512 handles of 40 buffers each took 14 s to
-// allocate once the previous 512 had been freed, against 0.35 s with one
-// block per handle).
-constexpr size_t kSlabFirst = (size_t)1 << 20;
-constexpr size_t kSlabMax = (size_t)64 << 20;
+// its small buffers from a few shared slabs: a pool that holds many freed
+// blocks makes every cudaMallocAsync slower (measured on B200: 512 handles
+// of 40 buffers each took 14 s to allocate once the previous 512 had been
+// freed, against 0.35 s with one block per handle).  Buffers of 64 KB or
+// more get blocks of their own size, so the slabs waste at most their
+// unused tail (under 1 MB).
+constexpr size_t kOwnBlock = (size_t)64 << 10;
+constexpr size_t kSlabFirst = (size_t)64 << 10;
+constexpr size_t kSlabMax = (size_t)1 << 20;
 constexpr size_t kAlign = 256;
 
 }  // namespace
@@ -71,6 +74,8 @@ struct mts_problem {
   int small_slab = -1;           // the slab small buffers are cut from
   size_t next_slab = kSlabFirst;  // size of the next small-buffer slab
   int64_t device_bytes = 0;       // sum of the slabs' sizes
+  bool sizing = false;            // grab only adds up sizes (the plan pass of finish_create)
+  size_t planned = 0;
   double* norm_part = nullptr;
   double* norm_out = nullptr;
   mts::SideStream side{nullptr, nullptr, nullptr};  // the mixed form's second stream
@@ -105,21 +110,25 @@ struct mts_problem {
     if (side.fork) cudaEventDestroy(side.fork);
     if (side.join) cudaEventDestroy(side.join);
   }
-  // bytes of device memory, 256-byte aligned, from the handle's slabs: a
-  // buffer at least as large as the next slab gets a slab of its own size;
-  // smaller ones are cut from the current small-buffer slab, and when that
-  // is full from a new one of twice its size (up to 64 MB)
+  // bytes of device memory, 256-byte aligned: a buffer of 64 KB or more
+  // gets a block of its own size; smaller ones are cut from the current
+  // small-buffer slab, and when that is full from a new one of twice its
+  // size (64 KB, then up to 1 MB)
   cudaError_t grab(size_t bytes, void** out) {
     *out = nullptr;
     bytes = (bytes + kAlign - 1) / kAlign * kAlign;
     if (bytes == 0) bytes = kAlign;
+    if (sizing) {
+      planned += bytes;
+      return cudaSuccess;
+    }
     if (small_slab >= 0 && slabs[small_slab].size - slabs[small_slab].used >= bytes) {
       Slab& sl = slabs[small_slab];
       *out = sl.base + sl.used;
       sl.used += bytes;
       return cudaSuccess;
     }
-    const bool own = bytes >= next_slab;
+    const bool own = bytes >= kOwnBlock;
     const size_t size = own ? bytes : next_slab;
     void* p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, size, stream);
@@ -133,11 +142,22 @@ struct mts_problem {
     *out = p;
     return cudaSuccess;
   }
+  // one block of `bytes` that the next grabs are cut from, whatever their size
+  cudaError_t reserve(size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+    if (e != cudaSuccess) return e;
+    slabs.push_back(Slab{(char*)p, bytes, 0});
+    device_bytes += (int64_t)bytes;
+    small_slab = (int)slabs.size() - 1;
+    return cudaSuccess;
+  }
   template <class T>
   cudaError_t put(T** dst, const T* src, size_t n) {
     if (n == 0) n = 1;
     cudaError_t e = grab(n * sizeof(T), (void**)dst);
-    if (e != cudaSuccess || !src) return e;
+    if (e != cudaSuccess || !src || sizing) return e;
     return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream);
   }
   // n elements (uploaded from src when given) followed by `pad` zeroed
@@ -145,7 +165,7 @@ struct mts_problem {
   template <class T>
   cudaError_t put_padded(T** dst, const T* src, size_t n, size_t pad) {
     cudaError_t e = grab((n + pad) * sizeof(T), (void**)dst);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || sizing) return e;
     e = cudaMemsetAsync(*dst + (src ? n : 0), 0, (src ? pad : n + pad) * sizeof(T), stream);
     if (e != cudaSuccess || !src) return e;
     return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream);
@@ -239,6 +259,19 @@ cudaError_t ensure_side_stream(mts_problem* h) {
 
 // Builds every device-side table of a problem from its grid, tags and
 // crossing list, and uploads them.
+// The device's pool keeps freed memory for the next allocations instead of
+// returning it to the driver at every synchronization (once per device,
+// before the first allocation of a handle or a device setup).
+void keep_pool(int device) {
+  static std::atomic<bool> kept[64];
+  if (device < 0 || device >= 64 || kept[device].exchange(true)) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+}
+
 mts_status finish_create(mts_problem* h) {
   const mts::Grid& g = h->g;
   const mts_params& p = h->prm;
@@ -453,17 +486,7 @@ mts_status finish_create(mts_problem* h) {
     }
   }
 
-  // the device's pool keeps freed memory for the next allocations instead of
-  // returning it to the driver at every synchronization (once per device)
-  static bool pool_kept[64] = {};
-  if (h->device >= 0 && h->device < 64 && !pool_kept[h->device]) {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) {
-      uint64_t keep = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    pool_kept[h->device] = true;
-  }
+  keep_pool(h->device);
   static bool configured = false;
   if (!configured) {
     mts::configure_kernels();
@@ -504,98 +527,114 @@ mts_status finish_create(mts_problem* h) {
   // row slack of the fields the sweeps stage whole chunks of: kRowPad rows of
   // the largest stride (an x-y plane)
   const size_t fpad = (size_t)mts::kRowPad * (size_t)g.nx * (size_t)g.ny;
-  CUDA_TRY(h->put_padded(&h->u0, (const double*)nullptr, (size_t)N, fpad));
-  CUDA_TRY(h->put_padded(&h->u1, (const double*)nullptr, (size_t)N, fpad));
-  D.u0 = h->u0;
-  D.u1 = h->u1;
-  CUDA_TRY(h->put_padded(&D.dp, (const double*)nullptr, (size_t)nmax * tmax, (size_t)mts::kRowPad * tmax));
-  for (int d = 0; d < 3; d++) {
-    for (int side = 0; side < 2; side++) {
-      double* pt = nullptr;
-      CUDA_TRY(h->put(&pt, ptab[d][side].data(), ptab[d][side].size()));
-      D.ptab[d][side] = pt;
-    }
-    double* rbk = nullptr;
-    CUDA_TRY(h->put(&rbk, (const double*)nullptr, 3 * blocks[d].size()));
-    D.rblk[d] = rbk;
-    D.nblk[d] = (int)blocks[d].size();
-    // per-node factor fields of the crossing lines (zero elsewhere), FP64
-    // and, for the mixed form, FP32 (1/bet and gam): filled on the device
-    double *fb = nullptr, *fg = nullptr;
-    float *fb32 = nullptr, *fg32 = nullptr;
-    if (!blocks[d].empty()) {
-      CUDA_TRY(h->put_padded(&fb, (const double*)nullptr, (size_t)N, fpad));
-      CUDA_TRY(h->put_padded(&fg, (const double*)nullptr, (size_t)N, fpad));
-      CUDA_TRY(h->put_padded(&fb32, (const float*)nullptr, (size_t)N, fpad));
-      CUDA_TRY(h->put_padded(&fg32, (const float*)nullptr, (size_t)N, fpad));
-    }
-    D.fbet[d] = fb;
-    D.fgam[d] = fg;
-    D.fib32[d] = fb32;
-    D.fgam32[d] = fg32;
-    // the same factors in FP32 for the mixed-precision sweeps, as 1/bet and gam
-    for (int side = 0; side < 2; side++) {
-      std::vector<float> p32(ptab[d][side].size());
-      for (size_t j = 0; j + 1 < p32.size(); j += 2) {
-        p32[j] = (float)(1.0 / ptab[d][side][j]);
-        p32[j + 1] = (float)ptab[d][side][j + 1];
+  // nodes that are a MIB row of some block: the pointwise passes leave them
+  // to a per-node pass over this list
+  std::vector<long long> mibn;
+  for (long long m = 0; m < N; m++)
+    if (tag8[(size_t)m] & (mts::TAG_MIBX | mts::TAG_MIBY | mts::TAG_MIBZ)) mibn.push_back(m);
+  h->norm_nb = mts::norms_blocks(D);
+  // Every buffer of the handle, placed twice: first only to add up their
+  // sizes, then into the one pool block of that size.
+  auto place_all = [&]() -> mts_status {
+    CUDA_TRY(h->put_padded(&h->u0, (const double*)nullptr, (size_t)N, fpad));
+    CUDA_TRY(h->put_padded(&h->u1, (const double*)nullptr, (size_t)N, fpad));
+    D.u0 = h->u0;
+    D.u1 = h->u1;
+    CUDA_TRY(h->put_padded(&D.dp, (const double*)nullptr, (size_t)nmax * tmax, (size_t)mts::kRowPad * tmax));
+    for (int d = 0; d < 3; d++) {
+      for (int side = 0; side < 2; side++) {
+        double* pt = nullptr;
+        CUDA_TRY(h->put(&pt, ptab[d][side].data(), ptab[d][side].size()));
+        D.ptab[d][side] = pt;
       }
-      float* pt = nullptr;
-      CUDA_TRY(h->put(&pt, p32.data(), p32.size()));
-      D.ptab32[d][side] = pt;
+      double* rbk = nullptr;
+      CUDA_TRY(h->put(&rbk, (const double*)nullptr, 3 * blocks[d].size()));
+      D.rblk[d] = rbk;
+      D.nblk[d] = (int)blocks[d].size();
+      // per-node factor fields of the crossing lines (zero elsewhere), FP64
+      // and, for the mixed form, FP32 (1/bet and gam): filled on the device
+      double *fb = nullptr, *fg = nullptr;
+      float *fb32 = nullptr, *fg32 = nullptr;
+      if (!blocks[d].empty()) {
+        CUDA_TRY(h->put_padded(&fb, (const double*)nullptr, (size_t)N, fpad));
+        CUDA_TRY(h->put_padded(&fg, (const double*)nullptr, (size_t)N, fpad));
+        CUDA_TRY(h->put_padded(&fb32, (const float*)nullptr, (size_t)N, fpad));
+        CUDA_TRY(h->put_padded(&fg32, (const float*)nullptr, (size_t)N, fpad));
+      }
+      D.fbet[d] = fb;
+      D.fgam[d] = fg;
+      D.fib32[d] = fb32;
+      D.fgam32[d] = fg32;
+      // the same factors in FP32 for the mixed-precision sweeps, as 1/bet and gam
+      for (int side = 0; side < 2; side++) {
+        std::vector<float> p32(ptab[d][side].size());
+        for (size_t j = 0; j + 1 < p32.size(); j += 2) {
+          p32[j] = (float)(1.0 / ptab[d][side][j]);
+          p32[j + 1] = (float)ptab[d][side][j + 1];
+        }
+        float* pt = nullptr;
+        CUDA_TRY(h->put(&pt, p32.data(), p32.size()));
+        D.ptab32[d][side] = pt;
+      }
+      float* rb32 = nullptr;
+      CUDA_TRY(h->put(&rb32, (const float*)nullptr, 3 * blocks[d].size()));
+      D.rblk32[d] = rb32;
     }
-    float* rb32 = nullptr;
-    CUDA_TRY(h->put(&rb32, (const float*)nullptr, 3 * blocks[d].size()));
-    D.rblk32[d] = rb32;
-  }
-  {
-    const size_t t32 = std::min((size_t)D.sweep_blocks * (size_t)mts::mixed_sweep_threads(),
-                                (size_t)maxlines + (size_t)mts::mixed_sweep_threads());
-    CUDA_TRY(h->put_padded(&D.r32, (const float*)nullptr, (size_t)N, fpad));
-    CUDA_TRY(h->put_padded(&D.dp32, (const float*)nullptr, (size_t)nmax * t32, (size_t)mts::kRowPad * t32));
-    D.precision = 0;
-  }
-  uint8_t* dtag = nullptr;
-  // (slack past the end: the fast form's bulk copies of tag rows may run
-  // past the last row of the last plane)
-  CUDA_TRY(h->put_padded(&dtag, tag8.data(), tag8.size(), fpad));
-  D.tag = dtag;
-  {
-    // nodes that are a MIB row of some block: the pointwise passes leave them
-    // to a per-node pass over this list
-    std::vector<long long> mibn;
-    for (long long m = 0; m < N; m++)
-      if (tag8[(size_t)m] & (mts::TAG_MIBX | mts::TAG_MIBY | mts::TAG_MIBZ)) mibn.push_back(m);
-    long long* dm = nullptr;
-    CUDA_TRY(h->put(&dm, mibn.empty() ? nullptr : mibn.data(), mibn.size()));
-    D.mibnode = dm;
-    D.nmibnode = (int)mibn.size();
-  }
-  for (int d = 0; d < 3; d++) {
-    uint8_t* ls = nullptr;
-    CUDA_TRY(h->put(&ls, lside[d].data(), lside[d].size()));
-    D.lside[d] = ls;
-  }
-  for (int d = 0; d < 3; d++) {
-    double *a = nullptr, *s = nullptr, *c = nullptr;
-    CUDA_TRY(h->put(&a, axv[d].data(), axv[d].size()));
-    CUDA_TRY(h->put(&s, s2v[d].data(), s2v[d].size()));
-    CUDA_TRY(h->put(&c, c2v[d].data(), c2v[d].size()));
-    D.ax[d] = a;
-    D.s2[d] = s;
-    D.c2[d] = c;
-    int32_t* bs = nullptr;
-    mts::MibBlock* bl = nullptr;
-    CUDA_TRY(h->put(&bs, bstart[d].data(), bstart[d].size()));
-    CUDA_TRY(h->put(&bl, blocks[d].empty() ? nullptr : blocks[d].data(), blocks[d].size()));
-    D.bstart[d] = bs;
-    D.blk[d] = bl;
-  }
-  mts::CrossConst* dcc = nullptr;
-  CUDA_TRY(h->put(&dcc, cc.empty() ? nullptr : cc.data(), cc.size()));
-  D.cc = dcc;
-  CUDA_TRY(h->put(&D.jv, (const double2*)nullptr, h->cross.size()));
-  CUDA_TRY(h->put(&D.status, (const int*)nullptr, 1));
+    {
+      const size_t t32 = std::min((size_t)D.sweep_blocks * (size_t)mts::mixed_sweep_threads(),
+                                  (size_t)maxlines + (size_t)mts::mixed_sweep_threads());
+      CUDA_TRY(h->put_padded(&D.r32, (const float*)nullptr, (size_t)N, fpad));
+      CUDA_TRY(h->put_padded(&D.dp32, (const float*)nullptr, (size_t)nmax * t32, (size_t)mts::kRowPad * t32));
+      D.precision = 0;
+    }
+    uint8_t* dtag = nullptr;
+    // (slack past the end: the fast form's bulk copies of tag rows may run
+    // past the last row of the last plane)
+    CUDA_TRY(h->put_padded(&dtag, tag8.data(), tag8.size(), fpad));
+    D.tag = dtag;
+    {
+      long long* dm = nullptr;
+      CUDA_TRY(h->put(&dm, mibn.empty() ? nullptr : mibn.data(), mibn.size()));
+      D.mibnode = dm;
+      D.nmibnode = (int)mibn.size();
+    }
+    for (int d = 0; d < 3; d++) {
+      uint8_t* ls = nullptr;
+      CUDA_TRY(h->put(&ls, lside[d].data(), lside[d].size()));
+      D.lside[d] = ls;
+    }
+    for (int d = 0; d < 3; d++) {
+      double *a = nullptr, *s = nullptr, *c = nullptr;
+      CUDA_TRY(h->put(&a, axv[d].data(), axv[d].size()));
+      CUDA_TRY(h->put(&s, s2v[d].data(), s2v[d].size()));
+      CUDA_TRY(h->put(&c, c2v[d].data(), c2v[d].size()));
+      D.ax[d] = a;
+      D.s2[d] = s;
+      D.c2[d] = c;
+      int32_t* bs = nullptr;
+      mts::MibBlock* bl = nullptr;
+      CUDA_TRY(h->put(&bs, bstart[d].data(), bstart[d].size()));
+      CUDA_TRY(h->put(&bl, blocks[d].empty() ? nullptr : blocks[d].data(), blocks[d].size()));
+      D.bstart[d] = bs;
+      D.blk[d] = bl;
+    }
+    mts::CrossConst* dcc = nullptr;
+    CUDA_TRY(h->put(&dcc, cc.empty() ? nullptr : cc.data(), cc.size()));
+    D.cc = dcc;
+    CUDA_TRY(h->put(&D.jv, (const double2*)nullptr, h->cross.size()));
+    CUDA_TRY(h->put(&D.status, (const int*)nullptr, 1));
+    CUDA_TRY(h->put(&h->norm_part, (const double*)nullptr, (size_t)3 * h->norm_nb));
+    CUDA_TRY(h->put(&h->norm_out, (const double*)nullptr, 3));
+    return MTS_OK;
+  };
+  h->sizing = true;
+  h->planned = 0;
+  mts_status placed = place_all();
+  h->sizing = false;
+  if (placed) return placed;
+  CUDA_TRY(h->reserve(h->planned));
+  placed = place_all();
+  if (placed) return placed;
   CUDA_TRY(cudaMemsetAsync(D.status, 0, sizeof(int), h->stream));
   {
     // the crossing lines' per-node factors; a zero pivot raises D.status
@@ -607,9 +646,6 @@ mts_status finish_create(mts_problem* h) {
     if (zero_pivot) return fail(MTS_ERR_ZERO_PIVOT, "zero pivot in a line factorisation");
     CUDA_TRY(cudaMemsetAsync(D.status, 0, sizeof(int), h->stream));
   }
-  h->norm_nb = mts::norms_blocks(D);
-  CUDA_TRY(h->put(&h->norm_part, (const double*)nullptr, (size_t)3 * h->norm_nb));
-  CUDA_TRY(h->put(&h->norm_out, (const double*)nullptr, 3));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->t = p.t0;
   return MTS_OK;
@@ -635,6 +671,9 @@ mts_status device_setup(const mts::Grid& g, const mts_surface& surf, const mts_p
                         std::vector<mts_crossing>& cross, mts::SetupReport* rep) {
   if (surf.kind != MTS_SURFACE_ELLIPSOID && surf.kind != MTS_SURFACE_TORUS)
     return fail(MTS_ERR_ARG, "unknown surface kind");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  keep_pool(dev);
   cudaStream_t st = nullptr;
   CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   std::string why;

@@ -22,8 +22,8 @@
 //                corner pairs, written at the line's offset, in the host's
 //                order (direction, line, left_loc);
 //   k_su_corner  one thread per MIB-L2 corner pair: the 36x36 system.
-// The LU matrices sit in global scratch (one slot per crossing or pair),
-// which is freed when the setup returns.
+// Each thread solves its systems in a slot of shared memory (LU updates are
+// serial chains of loads and stores, so they must not wait on L2).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -37,9 +37,20 @@ namespace {
 
 constexpr double kTolSetup = 1.0e-12;   // src/constant.h:10
 constexpr double kTolRtsafe = 1.0e-14;  // src/constant.h:11
-constexpr int kSlotL1 = 8 * 8;
-constexpr int kSlotL2 = 12 * 12;
-constexpr int kSlotCorner = 36 * 36;
+// An LU slot of order N holds, in doubles: A (N x N), B, x, the pivot
+// scales (N each) and the pivot rows (N ints); everything an LU works on
+// sits there, so the kernels keep no arrays of their own in local memory.
+template <int N>
+constexpr int slot_doubles() {
+  return (N * N + 3 * N + (N + 1) / 2 + 7) / 8 * 8;
+}
+constexpr int kSlotL1 = slot_doubles<8>();
+constexpr int kSlotL2 = slot_doubles<12>();
+constexpr int kSlotCorner = slot_doubles<36>();
+template <int N>
+__device__ __forceinline__ double* slot_b(double* s) { return s + N * N; }
+template <int N>
+__device__ __forceinline__ double* slot_x(double* s) { return s + N * N + N; }
 
 struct SurfD {
   int kind;
@@ -49,7 +60,7 @@ struct SurfD {
 // Stands for the reference's pow(v, 2).
 __device__ __forceinline__ double sqr(double v) { return v * v; }
 
-__device__ double lv_func(const SurfD& s, double x, double y, double z) {
+__device__ __forceinline__ double lv_func(const SurfD& s, double x, double y, double z) {
   if (s.kind == MTS_SURFACE_ELLIPSOID) {
     const double a = s.p[0], b = s.p[1], c = s.p[2], r = s.p[3];
     const double X = x - s.p[4], Y = y - s.p[5], Z = z - s.p[6];
@@ -59,7 +70,7 @@ __device__ double lv_func(const SurfD& s, double x, double y, double z) {
   return sqr(a - sqrt(x * x + y * y)) + z * z - b * b;
 }
 
-__device__ double lv_df(const SurfD& s, int axis, double x, double y, double z) {
+__device__ __forceinline__ double lv_df(const SurfD& s, int axis, double x, double y, double z) {
   if (s.kind == MTS_SURFACE_ELLIPSOID) {
     if (axis == 0) return 2 * (x - s.p[4]) / (s.p[0] * s.p[0]);
     if (axis == 1) return 2 * (y - s.p[5]) / (s.p[1] * s.p[1]);
@@ -71,7 +82,7 @@ __device__ double lv_df(const SurfD& s, int axis, double x, double y, double z) 
   return 2.0 * z;
 }
 
-__device__ void lv_normal(const SurfD& s, double x, double y, double z, double* n) {
+__device__ __forceinline__ void lv_normal(const SurfD& s, double x, double y, double z, double* n) {
   if (s.kind == MTS_SURFACE_ELLIPSOID) {
     const double a = s.p[0], b = s.p[1], c = s.p[2];
     const double X = x - s.p[4], Y = y - s.p[5], Z = z - s.p[6];
@@ -101,7 +112,7 @@ __device__ __forceinline__ double along_df(const SurfD& s, int axis, double v, d
 // Newton-Raphson safeguarded by bisection (Numerical Recipes rtsafe, as
 // Rtsafe_x/y/z); false when the bracket holds no sign change or 100
 // iterations do not converge.
-__device__ bool rtsafe(const SurfD& s, int axis, double v1, double v2, double p, double q, double* root) {
+__device__ __forceinline__ bool rtsafe(const SurfD& s, int axis, double v1, double v2, double p, double q, double* root) {
   double fl = along_f(s, axis, v1, p, q);
   double fh = along_f(s, axis, v2, p, q);
   if ((fl > 0.0 && fh > 0.0) || (fl < 0.0 && fh < 0.0)) return false;
@@ -160,7 +171,7 @@ __device__ bool rtsafe(const SurfD& s, int axis, double v1, double v2, double p,
 }
 
 // Gamma_x/y/z (surface_cartesian.cc:23-131).
-__device__ bool gamma_root(const SurfD& s, int axis, double v1, double v2, double p, double q, double* root) {
+__device__ __forceinline__ bool gamma_root(const SurfD& s, int axis, double v1, double v2, double p, double q, double* root) {
   if (!(v1 > v2) && !(v1 < v2)) return false;
   if (fabs(v1 - v2) < kTolRtsafe) {
     *root = (v1 + v2) / 2;
@@ -173,13 +184,13 @@ __device__ bool gamma_root(const SurfD& s, int axis, double v1, double v2, doubl
 // LU::LU, LU::solve and LU::det), on an N x N row-major matrix in place.
 template <int N>
 struct LuD {
-  double* a;
-  int indx[N];
+  double* a;     // N x N, row major, factored in place
+  double* vv;    // N pivot scales
+  int* indx;     // N pivot rows
   double d;
 
-  __device__ bool factor() {
+  __device__ __forceinline__ bool factor() {
     const double TINY = 1.0e-40;
-    double vv[N];
     d = 1.0;
     for (int i = 0; i < N; i++) {
       double big = 0.0, temp;
@@ -216,7 +227,7 @@ struct LuD {
     }
     return true;
   }
-  __device__ void solve(const double* b, double* x) const {
+  __device__ __forceinline__ void solve(const double* b, double* x) const {
     int ii = 0;
     for (int i = 0; i < N; i++) x[i] = b[i];
     for (int i = 0; i < N; i++) {
@@ -242,37 +253,47 @@ struct LuD {
   }
 };
 
-// Solves A x = B in place of A; returns 0 (no pivot row), 1 (solved) or
-// 2 (solved, |det| < TOL_SETUP: the reference's singular-matrix warning).
+// Solves A x = B of the slot (x into the slot); returns 0 (no pivot row),
+// 1 (solved) or 2 (solved, |det| < TOL_SETUP: the reference's
+// singular-matrix warning).
 template <int N>
-__device__ int lu_solve(double* A, const double* B, double* x) {
+__device__ __forceinline__ int lu_solve(double* slot) {
   LuD<N> lu;
-  lu.a = A;
+  lu.a = slot;
+  lu.vv = slot + N * N + 2 * N;
+  lu.indx = (int*)(slot + N * N + 3 * N);
   if (!lu.factor()) return 0;
-  lu.solve(B, x);
+  lu.solve(slot_b<N>(slot), slot_x<N>(slot));
   return fabs(lu.det()) < kTolSetup ? 2 : 1;
 }
 
 // Fornberg's finite-difference weights (Intersections::Weights,
-// intersection.cc:5093-5130) for m = 1: c is n x 2, row major.
-__device__ void fd_weights(double z, const double* x, int n, double* c) {
+// intersection.cc:5093-5130) for m = 1 on n points: c is n x 2, row major.
+template <int n>
+__device__ __forceinline__ void fd_weights(double z, const double* x, double* c) {
   const int m = 1, w = 2;
   double c1 = 1, c2, c3, c4 = x[0] - z, c5;
+#pragma unroll
   for (int i = 0; i < n; i++)
+#pragma unroll
     for (int j = 0; j < m + 1; j++) c[i * w + j] = 0;
   c[0] = 1;
+#pragma unroll
   for (int i = 1; i < n; i++) {
     const int mn = i < m ? i : m;
     c2 = 1;
     c5 = c4;
     c4 = x[i] - z;
+#pragma unroll
     for (int j = 0; j < i; j++) {
       c3 = x[i] - x[j];
       c2 = c2 * c3;
       if (j == i - 1) {
+#pragma unroll
         for (int k = mn; k > 0; k--) c[i * w + k] = c1 * (k * c[(i - 1) * w + k - 1] - c5 * c[(i - 1) * w + k]) / c2;
         c[i * w + 0] = -c1 * c5 * c[(i - 1) * w + 0] / c2;
       }
+#pragma unroll
       for (int k = mn; k > 0; k--) c[j * w + k] = (c4 * c[j * w + k] - k * c[j * w + k - 1]) / c3;
       c[j * w + 0] = c4 * c[j * w + 0] / c3;
     }
@@ -284,23 +305,27 @@ __device__ void fd_weights(double z, const double* x, int n, double* c) {
 struct Wei2 {
   double w[2][4];
 };
-__device__ Wei2 weights_table(double z, const double* v, int n) {
+template <int n>
+__device__ __forceinline__ Wei2 weights_table(double z, const double* v) {
   double temp[4 * 2];
-  fd_weights(z, v, n, temp);
+  fd_weights<n>(z, v, temp);
   Wei2 r;
+#pragma unroll
   for (int i = 0; i < 2; i++)
-    for (int j = 0; j < n; j++) r.w[i][j] = temp[j * 2 + i];
+#pragma unroll
+    for (int j = 0; j < 4; j++) r.w[i][j] = j < n ? temp[j * 2 + i] : 0.0;
   return r;
 }
 
 // MIB_L1 (intersection.cc:930-1066): the 8x8 system of one crossing.
-__device__ int mib_l1(double gamma, int id, double bi, double bo, double dv, double* A, double* x) {
+__device__ __forceinline__ int mib_l1(double gamma, int id, double bi, double bo, double dv, double* slot) {
   const int one = 4, tot = 8;
-  double B[tot];
+  double* A = slot;
+  double* B = slot_b<tot>(slot);
   for (int i = 0; i < tot * tot; i++) A[i] = 0.0;
   for (int i = 0; i < tot; i++) B[i] = 0.0;
   const double v[2] = {0, dv};
-  const Wei2 wt = weights_table(gamma, v, 2);
+  const Wei2 wt = weights_table<2>(gamma, v);
   const bool even = abs(id) % 2 == 0;
   int order = 0;
   B[0] = -wt.w[order][0];
@@ -326,14 +351,15 @@ __device__ int mib_l1(double gamma, int id, double bi, double bo, double dv, dou
     B[tot - 1] += -1;
   else
     B[tot - 1] += 1;
-  return lu_solve<8>(A, B, x);
+  return lu_solve<8>(slot);
 }
 
 // Irregular_MIB_L2 at second order (intersection.cc:1207-1395,
 // 1424-1470): the 12x12 system of one crossing.
-__device__ int mib_l2(double gamma, int id, double bi, double bo, double dv, double* A, double* x) {
+__device__ __forceinline__ int mib_l2(double gamma, int id, double bi, double bo, double dv, double* slot) {
   const int side = 2, st = 3, one = 6, tot = 12;
-  double B[tot];
+  double* A = slot;
+  double* B = slot_b<tot>(slot);
   for (int i = 0; i < tot * tot; i++) A[i] = 0.0;
   for (int i = 0; i < tot; i++) B[i] = 0.0;
   double vr[3], vl[3];
@@ -341,8 +367,8 @@ __device__ int mib_l2(double gamma, int id, double bi, double bo, double dv, dou
     vr[i] = -(side - 1) * dv + i * dv;
     vl[i] = (side - st + 1) * dv + i * dv;
   }
-  const Wei2 wr = weights_table(gamma, vr, st);
-  const Wei2 wl = weights_table(gamma, vl, st);
+  const Wei2 wr = weights_table<st>(gamma, vr);
+  const Wei2 wl = weights_table<st>(gamma, vl);
   const bool even = abs(id) % 2 == 0;
   int order = 0;
   for (int i = 0; i < side; i++) {
@@ -372,16 +398,17 @@ __device__ int mib_l2(double gamma, int id, double bi, double bo, double dv, dou
     B[tot - 1] += -1;
   else
     B[tot - 1] += 1;
-  return lu_solve<12>(A, B, x);
+  return lu_solve<12>(slot);
 }
 
 // Corner_MIB_L2_2nd + Get_cor_weights (intersection.cc:1479-1704,
 // 1752-1830): the 36x36 system of a corner pair L, R (consecutive
 // crossings of one line).
-__device__ int corner_l2(const mts_crossing& L, const mts_crossing& R, double bi, double bo, double dv, double* A,
-                         double* x) {
+__device__ __forceinline__ int corner_l2(const mts_crossing& L, const mts_crossing& R, double bi, double bo, double dv,
+                         double* slot) {
   const int one = 9, tot = 36, ns = 4;
-  double B[tot];
+  double* A = slot;
+  double* B = slot_b<tot>(slot);
   for (int i = 0; i < tot * tot; i++) A[i] = 0.0;
   for (int i = 0; i < tot; i++) B[i] = 0.0;
   auto a = [&](int i, int j) -> double& { return A[i * tot + j]; };
@@ -394,10 +421,10 @@ __device__ int corner_l2(const mts_crossing& L, const mts_crossing& R, double bi
   for (int i = 0; i < ns; i++) lvi[i] = i * dv;
   if ((dv - gl) > gr) lvi[ns - 1] = -dv;
   for (int i = 0; i < ns; i++) rvi[i] = lvi[i];
-  const Wei2 lo = weights_table(gl, lvo, ns);
-  const Wei2 li = weights_table(gl, lvi, ns);
-  const Wei2 ro = weights_table(dv + gr, rvo, ns);
-  const Wei2 ri = weights_table(dv + gr, rvi, ns);
+  const Wei2 lo = weights_table<ns>(gl, lvo);
+  const Wei2 li = weights_table<ns>(gl, lvi);
+  const Wei2 ro = weights_table<ns>(dv + gr, rvo);
+  const Wei2 ri = weights_table<ns>(dv + gr, rvi);
   const bool even = abs(L.id) % 2 == 0;
   // left interface, zero order
   int order = 0;
@@ -455,12 +482,12 @@ __device__ int corner_l2(const mts_crossing& L, const mts_crossing& R, double bi
     a(one * 3 + i, one * 3 + i) = -ri.w[order][3] * cin;
   }
   B[one * 3 + 8] = even ? -1 : 1;
-  return lu_solve<36>(A, B, x);
+  return lu_solve<36>(slot);
 }
 
 // Pmatrix_Setup_x/y/z (intersection.cc:2503-2598): the local frame, row
 // major, with the normal as its first row.
-__device__ void frame(int dir, const double* a, double* p) {
+__device__ __forceinline__ void frame(int dir, const double* a, double* p) {
   for (int i = 0; i < 3; i++) p[i] = a[i];
   if (dir == 0) {
     p[3] = a[2] / sqrt(a[0] * a[0] + a[2] * a[2]);
@@ -498,8 +525,6 @@ struct SetupArgs {
   uint8_t* lerr;        // the scan of this line fails
   int* offs;            // exclusive sum of counts; offs[total lines] = all
   mts_crossing* out;
-  double* scratch;      // LU slots: one per crossing (singles, L1 corners)
-  double* cscratch;     // one per MIB-L2 corner pair
   int* corner_list;     // offsets of the left crossings of MIB-L2 pairs
   int* ctrl;            // [0] node on the interface, [1] corner pairs, [2] L2 pairs listed,
                         // [3] first failing line (INT_MAX: none), [4] its status
@@ -540,12 +565,18 @@ __device__ __forceinline__ void line_of(const SetupArgs& A, long long l, int& d,
   i2 = 1 + (int)(l % w);
 }
 
+// Node indices of row j of line (d, i1, i2): the line's fixed axes are
+// (y, z) for x lines, (x, z) for y lines and (x, y) for z lines.
+__device__ __forceinline__ void node_ijk(int d, int i1, int i2, int j, int& ix, int& iy, int& iz) {
+  ix = d == 0 ? j : i1;
+  iy = d == 0 ? i1 : d == 1 ? j : i2;
+  iz = d == 2 ? j : i2;
+}
+
 __device__ __forceinline__ long long node_of(const SetupArgs& A, int d, int i1, int i2, int j) {
-  int idx[3];
-  idx[d == 0 ? 1 : 0] = i1;
-  idx[d == 2 ? 1 : 2] = i2;
-  idx[d] = j;
-  return (long long)idx[0] + (long long)A.n[0] * ((long long)idx[1] + (long long)A.n[1] * idx[2]);
+  int ix, iy, iz;
+  node_ijk(d, i1, i2, j, ix, iy, iz);
+  return (long long)ix + (long long)A.n[0] * ((long long)iy + (long long)A.n[1] * iz);
 }
 
 __global__ void k_su_count(const SetupArgs A, long long total_lines) {
@@ -615,7 +646,7 @@ __global__ void __launch_bounds__(1024) k_su_scan(const int* __restrict__ counts
   if (threadIdx.x == 1023) offs[n] = (int)part[1023];
 }
 
-__device__ void note_failure(const SetupArgs& A, long long l, int status) {
+__device__ __forceinline__ void note_failure(const SetupArgs& A, long long l, int status) {
   // the first failing line in line order decides the status, as in one pass
   const int prev = atomicMin(&A.ctrl[kCtrlFirstBad], (int)l);
   (void)prev;
@@ -624,26 +655,28 @@ __device__ void note_failure(const SetupArgs& A, long long l, int status) {
 
 // Root, coordinates, normal and frame of the crossing in cell [j, j+1] of
 // line (d, i1, i2); the record's other fields stay zero.
-__device__ bool locate(const SetupArgs& A, int d, int i1, int i2, int j, int id, mts_crossing* c) {
-  const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
-  const double* v = A.ax[d];
+__device__ __forceinline__ bool locate(const SetupArgs& A, int d, int i1, int i2, int j, int id, mts_crossing* c) {
+  const double* v = d == 0 ? A.ax[0] : d == 1 ? A.ax[1] : A.ax[2];
+  const double fp = d == 0 ? A.ax[1][i1] : A.ax[0][i1];
+  const double fq = d == 2 ? A.ax[1][i2] : A.ax[2][i2];
   double root;
-  if (!gamma_root(A.s, d, v[j], v[j + 1], A.ax[a1][i1], A.ax[a2][i2], &root)) return false;
-  int idx[3];
-  idx[a1] = i1;
-  idx[a2] = i2;
-  idx[d] = j;
+  if (!gamma_root(A.s, d, v[j], v[j + 1], fp, fq, &root)) return false;
+  int ix, iy, iz;
+  node_ijk(d, i1, i2, j, ix, iy, iz);
   c->dir = d;
   c->indx1 = i1;
   c->indx2 = i2;
   c->id = id;
   c->left_loc = j;
-  double co[3] = {A.ax[0][idx[0]], A.ax[1][idx[1]], A.ax[2][idx[2]]};
-  co[d] = root;
-  for (int k = 0; k < 3; k++) c->coord[k] = co[k];
-  c->gamma = co[d] - v[j];
+  const double cx = d == 0 ? root : A.ax[0][ix];
+  const double cy = d == 1 ? root : A.ax[1][iy];
+  const double cz = d == 2 ? root : A.ax[2][iz];
+  c->coord[0] = cx;
+  c->coord[1] = cy;
+  c->coord[2] = cz;
+  c->gamma = root - v[j];
   double nrm[3], p[9];
-  lv_normal(A.s, co[0], co[1], co[2], nrm);
+  lv_normal(A.s, cx, cy, cz, nrm);
   frame(d, nrm, p);
   for (int k = 0; k < 3; k++) c->normal[k] = nrm[k];
   for (int k = 0; k < 9; k++) c->p[k] = p[k];
@@ -654,7 +687,11 @@ __device__ __forceinline__ void count_singular(const SetupArgs& A, int r) {
   if (r == 2) atomicAdd(A.singular, 1ULL);
 }
 
-__global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long total_lines) {
+constexpr int kCrossThreads = 32;  // x one LU slot of shared memory each: 48 KB at MIB-L2
+
+__global__ void __launch_bounds__(kCrossThreads) k_su_cross(const SetupArgs A, long long total_lines) {
+  extern __shared__ double su_smem[];
+  double* const M = su_smem + threadIdx.x * (A.mib == 1 ? kSlotL1 : kSlotL2);
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < total_lines;
        l += (long long)gridDim.x * blockDim.x) {
     if (A.counts[l] == 0 && !A.lerr[l]) continue;
@@ -665,10 +702,8 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
     auto tag = [&](int j) { return (int)A.tags[s0 + st * j]; };
     const int nd = A.n[d];
     const double dv = A.h[d];
-    const int slot = A.mib == 1 ? kSlotL1 : kSlotL2;
     int k = A.offs[l];
     int ifp = 0, j = 1, status = 0;
-    double x[12];
     while (j < nd - 1) {
       if (tag(j) * tag(j + 1) < 0) {
         if (j + 2 >= nd) {
@@ -682,9 +717,9 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
             status = MTS_ERR_NONFINITE;
             break;
           }
-          double* M = A.scratch + (size_t)k * slot;
           if (A.mib == 1) {
-            const int r = mib_l1(c->gamma, c->id, A.bi, A.bo, dv, M, x);
+            const int r = mib_l1(c->gamma, c->id, A.bi, A.bo, dv, M);
+            const double* x = slot_x<8>(M);
             if (!r) {
               status = MTS_ERR_SETUP;
               break;
@@ -700,7 +735,8 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
             c->weir[4] = x[6];
             c->weir[5] = x[7];
           } else {
-            const int r = mib_l2(c->gamma, c->id, A.bi, A.bo, dv, M, x);
+            const int r = mib_l2(c->gamma, c->id, A.bi, A.bo, dv, M);
+            const double* x = slot_x<12>(M);
             if (!r) {
               status = MTS_ERR_SETUP;
               break;
@@ -733,8 +769,8 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
           }
           if (A.mib == 1) {
             // Corner_MIB_L1 (intersection.cc:1128-1200): each crossing alone
-            double* M = A.scratch + (size_t)k * slot;
-            const int r1 = mib_l1(L->gamma, L->id, A.bi, A.bo, dv, M, x);
+            const int r1 = mib_l1(L->gamma, L->id, A.bi, A.bo, dv, M);
+            const double* x = slot_x<8>(M);
             if (!r1) {
               status = MTS_ERR_SETUP;
               break;
@@ -749,7 +785,7 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
             L->weir[2] = x[5];
             L->weir[5] = x[6];
             L->weir[6] = x[7];
-            const int r2 = mib_l1(R->gamma, R->id, A.bi, A.bo, dv, M, x);
+            const int r2 = mib_l1(R->gamma, R->id, A.bi, A.bo, dv, M);
             if (!r2) {
               status = MTS_ERR_SETUP;
               break;
@@ -778,14 +814,17 @@ __global__ void __launch_bounds__(128) k_su_cross(const SetupArgs A, long long t
   }
 }
 
-__global__ void __launch_bounds__(64) k_su_corner(const SetupArgs A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One thread per CTA, its 36x36 slot (11.4 KB) in shared memory.
+__global__ void __launch_bounds__(1) k_su_corner(const SetupArgs A) {
+  extern __shared__ double su_smem[];
+  const int i = blockIdx.x;
   if (i >= A.ctrl[kCtrlListed]) return;
   const int k = A.corner_list[i];
   mts_crossing* L = A.out + k;
   mts_crossing* R = L + 1;
-  double x[36];
-  const int r = corner_l2(*L, *R, A.bi, A.bo, A.h[L->dir], A.cscratch + (size_t)i * kSlotCorner, x);
+  double* M = su_smem;
+  const int r = corner_l2(*L, *R, A.bi, A.bo, A.h[L->dir], M);
+  const double* x = slot_x<36>(M);
   if (!r) {
     const int d = L->dir;
     long long l = (long long)(L->indx1 - 1) * (A.n[d == 2 ? 1 : 2] - 2) + (L->indx2 - 1);
@@ -807,7 +846,7 @@ __global__ void __launch_bounds__(64) k_su_corner(const SetupArgs A) {
 int grid_for(long long work, int threads) {
   long long b = (work + threads - 1) / threads;
   if (b < 1) b = 1;
-  if (b > 148LL * 16) b = 148LL * 16;
+  if (b > 148LL * 64) b = 148LL * 64;
   return (int)b;
 }
 
@@ -904,19 +943,17 @@ mts_status setup_on_device(const Grid& g, const mts_surface& surf, double beta_i
   }
   const int corners = ctrl[kCtrlCorners];
 
-  // second allocation: the records, the LU slots, the corner pairs' slots and list
+  // second allocation: the records and the list of MIB-L2 corner pairs
   const size_t b_out = ((size_t)total * sizeof(mts_crossing) + 255) / 256 * 256;
-  const size_t b_scr = (size_t)total * (mib == 1 ? kSlotL1 : kSlotL2) * 8;
   const size_t ncs = mib == 2 ? (size_t)corners : 0;
   char* base2 = nullptr;
-  SU_TRY(alloc(b_out + b_scr + ncs * kSlotCorner * 8 + ncs * 4, (void**)&base2), "allocation");
+  SU_TRY(alloc(b_out + ncs * 4, (void**)&base2), "allocation");
   A.out = (mts_crossing*)base2;
-  A.scratch = (double*)(base2 + b_out);
-  A.cscratch = (double*)(base2 + b_out + b_scr);
-  A.corner_list = (int*)(base2 + b_out + b_scr + ncs * kSlotCorner * 8);
+  A.corner_list = (int*)(base2 + b_out);
   SU_TRY(cudaMemsetAsync(A.out, 0, (size_t)total * sizeof(mts_crossing), st), "clear");
-  k_su_cross<<<grid_for(total_lines, 128), 128, 0, st>>>(A, total_lines);
-  if (mib == 2 && corners > 0) k_su_corner<<<(corners + 63) / 64, 64, 0, st>>>(A);
+  const size_t cross_smem = (size_t)kCrossThreads * (mib == 1 ? kSlotL1 : kSlotL2) * sizeof(double);
+  k_su_cross<<<grid_for(total_lines, kCrossThreads), kCrossThreads, cross_smem, st>>>(A, total_lines);
+  if (mib == 2 && corners > 0) k_su_corner<<<corners, 1, kSlotCorner * sizeof(double), st>>>(A);
   SU_TRY(cudaGetLastError(), "launch");
   unsigned long long singular = 0;
   SU_TRY(cudaMemcpyAsync(ctrl, A.ctrl, sizeof ctrl, cudaMemcpyDeviceToHost, st), "control read");
