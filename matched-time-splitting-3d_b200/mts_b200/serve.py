@@ -72,7 +72,7 @@ class Server:
     setup: "host" (tags, crossings and MIB weights on the pool's host
       threads) or "device" (the same on the GPU, mts_setup_device)."""
 
-    def __init__(self, hbm_budget: float = 120e9, chunk_steps: int = 8, host_threads: int = 16,
+    def __init__(self, hbm_budget: float = 120e9, chunk_steps: int = 32, host_threads: int = 16,
                  keep_solutions: bool = False, precision: str = "plain", max_active: int = 256,
                  setup: str = "host"):
         self.budget = int(hbm_budget)
