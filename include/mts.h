@@ -198,6 +198,15 @@ mts_status mts_norms(mts_handle h, double* lmax, double* l2, int32_t* argmax3);
 mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double* lmax, double* l2,
                              int32_t* argmax3);
 
+/* The fictitious points' error report at the current time: Refresh_Fp
+ * (src/spatial/intersection.cc:1841-2281) on the device, one thread per
+ * crossing or corner pair, and Error_Fp's maximum and root mean square of
+ * the relative errors (:4667-4771), added up on the host in its loop order:
+ * the reference's values bit for bit (inf or NaN where the exact solution of
+ * the other side is 0 at a fictitious point's node, as there).  The reference
+ * prints them with 4 digits ("Lmax = ...", "L2   = ..."). */
+mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2);
+
 mts_status mts_get_time(mts_handle h, double* t);
 mts_status mts_set_time(mts_handle h, double t);
 

@@ -163,6 +163,23 @@ class GpuStepper {
     out << std::fixed << std::endl;
   }
 
+  // In place of the reference's report pair
+  //   inter.Refresh_Fp(eq); inter.Error_Fp(out);   (helper.h:230-231)
+  // the fictitious points' errors at the stepper's time, evaluated on the
+  // device (mts_fp_errors), written in Error_Fp's text
+  // (intersection.cc:4763-4770).
+  void Error_Fp(Equation& e, std::ofstream& out) {
+    check_equation(mesh_, e, eq_, bi_, bo_, t_);
+    create();
+    double lmax, l2;
+    check(mts_fp_errors(h_, &lmax, &l2));
+    out << "------------------------ Error of FPs ------------------------" << std::endl;
+    out << std::setprecision(3) << std::scientific;
+    out << "Lmax = " << lmax << std::endl;
+    out << "L2   = " << l2 << std::endl;
+    out << std::fixed << std::endl;
+  }
+
   mts_handle handle() const { return h_; }
 
  private:

@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmts_b200.so")
-SOURCES = ["setup.cpp", "setup_gpu.cu", "kernels.cu", "mixed.cu", "fast.cu", "capi.cu"]
+SOURCES = ["setup.cpp", "setup_gpu.cu", "kernels.cu", "mixed.cu", "fast.cu", "diag.cu", "capi.cu"]
 HEADERS = ["setup.h", "device.h", "device_common.cuh"]
 OBJ_DIR = os.path.join(HERE, "build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -79,6 +79,12 @@ struct mts_problem {
   double* norm_part = nullptr;
   double* norm_out = nullptr;
   mts::SideStream side{nullptr, nullptr, nullptr};  // the mixed form's second stream
+  // the fictitious points' error report (mts_fp_errors), built on first use
+  mts_crossing* fp_cr = nullptr;
+  int32_t* fp_ci = nullptr;
+  int8_t* fp_role = nullptr;
+  double* fp_err = nullptr;
+  std::vector<int32_t> fp_perm;
 
   int norm_nb = 1;
   double t = 0;
@@ -1157,6 +1163,70 @@ mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double
     argmax3[0] = (int32_t)(key / h->g.ny);
   }
   return st;
+}
+
+mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  const int n = (int)h->cross.size();
+  if (n > 0 && !h->fp_cr) {
+    // the records sorted by (direction, line, position), the order of
+    // Refresh_Fp's and Error_Fp's loops within a direction
+    std::vector<int32_t>& perm = h->fp_perm;
+    perm.resize((size_t)n);
+    for (int i = 0; i < n; i++) perm[(size_t)i] = i;
+    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) {
+      const mts_crossing &x = h->cross[(size_t)a], &y = h->cross[(size_t)b];
+      if (x.dir != y.dir) return x.dir < y.dir;
+      if (x.indx1 != y.indx1) return x.indx1 < y.indx1;
+      if (x.indx2 != y.indx2) return x.indx2 < y.indx2;
+      return x.left_loc < y.left_loc;
+    });
+    std::vector<mts_crossing> rec((size_t)n);
+    std::vector<int8_t> role((size_t)n, 0);
+    for (int i = 0; i < n; i++) rec[(size_t)i] = h->cross[(size_t)perm[(size_t)i]];
+    for (int i = 0; i < n;) {
+      if (rec[(size_t)i].id > 0) {
+        i += 1;
+        continue;
+      }
+      if (i + 1 >= n || rec[(size_t)i + 1].id >= 0 || rec[(size_t)i + 1].dir != rec[(size_t)i].dir ||
+          rec[(size_t)i + 1].indx1 != rec[(size_t)i].indx1 || rec[(size_t)i + 1].indx2 != rec[(size_t)i].indx2)
+        return fail(MTS_ERR_SETUP, "a corner crossing without its pair on the same line");
+      role[(size_t)i] = 1;
+      role[(size_t)i + 1] = 2;
+      i += 2;
+    }
+    CUDA_TRY(h->put(&h->fp_cr, rec.data(), rec.size()));
+    CUDA_TRY(h->put(&h->fp_ci, perm.data(), perm.size()));
+    CUDA_TRY(h->put(&h->fp_role, role.data(), role.size()));
+    CUDA_TRY(h->put(&h->fp_err, (const double*)nullptr, 2 * (size_t)n));
+  }
+  std::vector<double> err(2 * (size_t)n);
+  if (n > 0) {
+    h->launches += mts::launch_fp_errors(h->dev, h->fp_cr, h->fp_ci, h->fp_role, n, std::exp(-h->t), h->fp_err,
+                                         h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(err.data(), h->fp_err, err.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  mts_status st = sync_status(h);
+  if (st != MTS_OK) return st;
+  // Error_Fp's loops: directions z, y, x; per crossing its left error, then
+  // its right one
+  double fmax = 0, sum = 0;
+  long long no = 0;
+  for (int d = 2; d >= 0; d--)
+    for (int i = 0; i < n; i++) {
+      if (h->cross[(size_t)h->fp_perm[(size_t)i]].dir != d) continue;
+      const double el = err[2 * (size_t)i], er = err[2 * (size_t)i + 1];
+      no += 2;
+      sum += el * el;
+      sum += er * er;
+      if (std::abs(el) > fmax) fmax = std::abs(el);
+      if (std::abs(er) > fmax) fmax = std::abs(er);
+    }
+  if (lmax) *lmax = fmax;
+  if (l2) *l2 = std::sqrt(sum / (double)no);
+  return MTS_OK;
 }
 
 mts_status mts_get_time(mts_handle h, double* t) {

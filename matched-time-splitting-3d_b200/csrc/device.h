@@ -25,6 +25,8 @@
 
 #include <cstdint>
 
+#include "../../include/mts.h"
+
 namespace mts {
 
 enum : uint8_t { TAG_OUT = 1, TAG_MIBX = 2, TAG_MIBY = 4, TAG_MIBZ = 8 };
@@ -235,6 +237,13 @@ void launch_tick(const Dev& P, cudaStream_t stream);  // ++(*P.tstep)
 unsigned pointwise_rows_grid(const Dev& P);
 constexpr int kProfileSlots = 8;
 constexpr int kRowPad = 16;  // rows of slack after each staged field (>= chunk rows)
+// The fictitious points' relative errors (Refresh_Fp): two per crossing
+// into err, for the records cr sorted by (direction, line, position) whose
+// indices in the handle's list are ci; role[i] 0 single, 1 left of a corner
+// pair, 2 its right (diag.cu).
+int launch_fp_errors(const Dev& P, const mts_crossing* cr, const int32_t* ci, const int8_t* role, int n, double E,
+                     double* err, cudaStream_t stream);
+
 int launch_norms(const Dev& P, double E, const double* u, double* partial, int nblocks,
                  double* out3, cudaStream_t stream);
 int norms_blocks(const Dev& P);

@@ -288,6 +288,14 @@ class Solver:
         check(self._L.mts_autotune(self._h, int(steps), out.ctypes.data), "mts_autotune")
         return tuple(int(v) for v in out)
 
+    def fp_errors(self):
+        """The fictitious points' error report at the current time
+        (mts_fp_errors: Refresh_Fp + Error_Fp on the device): (L-infinity,
+        root mean square) of their relative errors."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(self._L.mts_fp_errors(self._h, ctypes.byref(a), ctypes.byref(b)), "mts_fp_errors")
+        return a.value, b.value
+
     def stream(self) -> int:
         v = ctypes.c_void_p()
         check(self._L.mts_get_stream(self._h, ctypes.byref(v)), "mts_get_stream")

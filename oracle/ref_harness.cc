@@ -168,6 +168,7 @@ struct Args {
   double t_end = 1.0;
   string dump_u, dump_tags, dump_mib, dump_u0;
   string report;     // --report F: the stepper's own Error() text at the end
+  string fp_errors;  // --fp-errors F: Refresh_Fp + Error_Fp at the end (values in binary, then the text)
   bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
   int beta_plugin = -1;  // --beta-plugin 1: the reference's Beta_1 instead of the piecewise-constant beta
 };
@@ -178,7 +179,7 @@ struct Args {
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
           "        --beta bi bo [--beta-plugin 1] --eq 0|3|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
-          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F]\n"
+          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F] [--fp-errors F]\n"
 #ifdef MTS_DROPIN
           "        [--gpu]\n"
 #endif
@@ -247,6 +248,9 @@ Args parse(int argc, char** argv) {
     } else if (k == "--report") {
       need(1);
       a.report = argv[++i];
+    } else if (k == "--fp-errors") {
+      need(1);
+      a.fp_errors = argv[++i];
 #ifdef MTS_DROPIN
     } else if (k == "--gpu") {
       a.gpu = true;
@@ -469,6 +473,11 @@ int main(int argc, char** argv) {
         run(st, lod_step);
       else
         run(st, ts_step);
+      if (!a.fp_errors.empty()) {
+        // the device's fictitious-point report, beside the reference's below
+        ofstream o(a.fp_errors + ".gpu");
+        st.Error_Fp(*make_eq(a, t_now, beta), o);
+      }
     } catch (const std::exception& e) {
       fprintf(stderr, "mts_dropin: %s\n", e.what());
       return 3;
@@ -487,6 +496,42 @@ int main(int argc, char** argv) {
   }
   norms(*make_eq(a, t_now, beta));
   if (!a.dump_u.empty()) dump_field(a.dump_u, uh, nx, ny, nz);
+  if (!a.fp_errors.empty()) {
+    // The fictitious points' errors against the exact solution at the final
+    // time, as the reference's time loops report them (helper.h:230-231):
+    // Refresh_Fp, then Error_Fp's maximum and root mean square recomputed
+    // here in its loop order (intersection.cc:4667-4771) so that the values
+    // stay in binary, followed by Error_Fp's own text.
+    inter.Refresh_Fp(*make_eq(a, t_now, beta));
+    double fmax = 0, fsum = 0;
+    long long fno = 0;
+    auto add = [&](Intersection_Data& d) {
+      for (size_t i = 0; i < d.err.errr.size(); i++) {
+        fno += 2;
+        fsum += d.err.errl[i] * d.err.errl[i];
+        fsum += d.err.errr[i] * d.err.errr[i];
+        if (fabs(d.err.errl[i]) > fmax) fmax = fabs(d.err.errl[i]);
+        if (fabs(d.err.errr[i]) > fmax) fmax = fabs(d.err.errr[i]);
+      }
+    };
+    for (int ix = 1; ix < nx - 1; ix++)
+      for (int iy = 1; iy < ny - 1; iy++)
+        for (auto& d : inter.ifpz[ix][iy])
+          if (d.ID != 0) add(d);
+    for (int ix = 1; ix < nx - 1; ix++)
+      for (int iz = 1; iz < nz - 1; iz++)
+        for (auto& d : inter.ifpy[ix][iz])
+          if (d.ID != 0) add(d);
+    for (int iy = 1; iy < ny - 1; iy++)
+      for (int iz = 1; iz < nz - 1; iz++)
+        for (auto& d : inter.ifpx[iy][iz])
+          if (d.ID != 0) add(d);
+    FILE* f = fopen(a.fp_errors.c_str(), "w");
+    fprintf(f, "%.17g %.17g %.17g %lld\n", fmax, sqrt(fsum / fno), fsum, fno);
+    fclose(f);
+    ofstream txt(a.fp_errors, ios::app);
+    inter.Error_Fp(txt);
+  }
 
   printf(
       "{\"nx\": %d, \"ny\": %d, \"nz\": %d, \"steps\": %d, \"t\": %.17g, \"lmax\": %.17g, "

@@ -73,3 +73,21 @@ def test_dropin_gpu_equals_reference_bitwise(name, prob, tmp_path):
     ref_rep = (tmp_path / "ref.txt").read_text()
     assert ref_rep.startswith("[Xmax,Ymax,Zmax] = [")
     assert (tmp_path / "gpu.txt").read_text() == ref_rep
+
+
+@pytest.mark.gpu
+@needs_dropin
+@pytest.mark.parametrize("mib", [1, 2])
+def test_dropin_fp_error_report(mib, tmp_path):
+    """The stepper's Error_Fp (the device's Refresh_Fp + Error_Fp) writes the
+    same report as the reference's Intersections::Error_Fp in the same run."""
+    prob = O.Problem(n=(26, 30, 28), surface="ellipsoid", surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
+                     beta_in=1.0, beta_out=100.0, method="adi", mib=mib, dt=1.0 / 16, steps=3)
+    f = tmp_path / "fp.txt"
+    cp = subprocess.run([O.REF_BIN_DROPIN, *prob.ref_args(), "--gpu", "--fp-errors", str(f)], capture_output=True,
+                        text=True, timeout=300)
+    assert cp.returncode == 0, cp.stderr
+    ref_text = "\n".join(f.read_text().splitlines()[1:])
+    gpu_text = (tmp_path / "fp.txt.gpu").read_text()
+    assert "Error of FPs" in ref_text and "inf" not in ref_text and "nan" not in ref_text
+    assert gpu_text.strip() == ref_text.strip()
