@@ -43,6 +43,10 @@
 #include "mts_reference_adapter.hpp"
 #endif
 
+// The reference's Write_txt (ref_write_txt.cc).
+void ref_write_txt(Intersections& inter, Mesh& mesh, Beta& beta, CubicDoub& uh, int equation, double t);
+
+
 using namespace std;
 
 namespace {
@@ -168,6 +172,7 @@ struct Args {
   double t_end = 1.0;
   string dump_u, dump_tags, dump_mib, dump_u0;
   string report;     // --report F: the stepper's own Error() text at the end
+  bool write_txt = false;  // --write-txt: the reference's Write_txt files (Eq_0..Eq_7) at the end
   string fp_errors;  // --fp-errors F: Refresh_Fp + Error_Fp at the end (values in binary, then the text)
   bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
   int beta_plugin = -1;  // --beta-plugin 1: the reference's Beta_1 instead of the piecewise-constant beta
@@ -179,7 +184,7 @@ struct Args {
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
           "        --beta bi bo [--beta-plugin 1] --eq 0|3|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
-          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F] [--fp-errors F]\n"
+          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F] [--fp-errors F] [--write-txt]\n"
 #ifdef MTS_DROPIN
           "        [--gpu]\n"
 #endif
@@ -248,6 +253,8 @@ Args parse(int argc, char** argv) {
     } else if (k == "--report") {
       need(1);
       a.report = argv[++i];
+    } else if (k == "--write-txt") {
+      a.write_txt = true;
     } else if (k == "--fp-errors") {
       need(1);
       a.fp_errors = argv[++i];
@@ -496,6 +503,13 @@ int main(int argc, char** argv) {
   }
   norms(*make_eq(a, t_now, beta));
   if (!a.dump_u.empty()) dump_field(a.dump_u, uh, nx, ny, nz);
+  if (a.write_txt) {
+    if (a.eq > 7) {
+      fprintf(stderr, "--write-txt: the reference's Write_txt knows Eq_0..Eq_7 only\n");
+      return 2;
+    }
+    ref_write_txt(inter, mesh, beta, uh, a.eq, t_now);
+  }
   if (!a.fp_errors.empty()) {
     // The fictitious points' errors against the exact solution at the final
     // time, as the reference's time loops report them (helper.h:230-231):

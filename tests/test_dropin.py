@@ -91,3 +91,26 @@ def test_dropin_fp_error_report(mib, tmp_path):
     gpu_text = (tmp_path / "fp.txt.gpu").read_text()
     assert "Error of FPs" in ref_text and "inf" not in ref_text and "nan" not in ref_text
     assert gpu_text.strip() == ref_text.strip()
+
+
+@pytest.mark.gpu
+@needs_dropin
+@pytest.mark.parametrize("method", ["adi", "lod-ie", "ts"])
+def test_dropin_write_txt_files_match(method, tmp_path):
+    """The reference's own near-interface dump (Write_txt, helper.h:442-575:
+    the closest outside node of every crossing, its value and its error)
+    written from the drop-in's field is byte for byte the file written from
+    the reference stepper's.  Write_txt knows the reference's Eq_0..Eq_7
+    only, so the run uses Eq_0."""
+    prob = O.Problem(n=(21, 19, 23), surface="ellipsoid", surface_params=(0.55, 0.6, 0.45, 1.0, -0.04, 0.03, 0.01),
+                     beta_in=1.0, beta_out=0.01, eq=0, method=method, mib=2, dt=0.1, steps=3)
+    out = {}
+    for arm, extra in (("ref", []), ("gpu", ["--gpu"])):
+        d = tmp_path / arm
+        d.mkdir()
+        cp = subprocess.run([O.REF_BIN_DROPIN, *prob.ref_args(), "--write-txt", *extra], capture_output=True,
+                            text=True, timeout=300, cwd=str(d))
+        assert cp.returncode == 0, cp.stderr
+        out[arm] = [(d / f).read_bytes() for f in ("Numerical Solutions.txt", "Numerical Error.txt")]
+    assert out["ref"][0].count(b"\n") > 100
+    assert out["gpu"] == out["ref"]
