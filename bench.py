@@ -114,10 +114,11 @@ def parse():
 # device state and host work included; the GPU is synchronized at both ends).
 
 def run_precision(grids=(257, 385), betas=(1e-3, 1.0, 1e3), steps: int = 20) -> dict:
-    """The precision form against the plain form: Douglas-ADI + MIB-L2, torus,
-    beta_out / beta_in in `betas`, dt = h, `steps` steps of each from the same
-    start; cell-steps/s of both (CUDA events), L-infinity of both against the
-    exact solution, and the mixed solution's difference from the plain one."""
+    """The precision form against both FP64 forms: Douglas-ADI + MIB-L2,
+    torus, beta_out / beta_in in `betas`, dt = h, `steps` steps of each from
+    the same start; cell-steps/s of each (CUDA events), L-infinity of each
+    against the exact solution, and the mixed solution's difference from the
+    bit-exact one."""
     import numpy as np
     import torch
 
@@ -127,9 +128,9 @@ def run_precision(grids=(257, 385), betas=(1e-3, 1.0, 1e3), steps: int = 20) -> 
     for n in grids:
         for b in betas:
             spec = M.Spec(n=(n, n, n), surface="torus", surface_params=(0.5, 0.2), beta_in=1.0, beta_out=b,
-                          method="adi", mib=2, dt=2.0 / (n - 1))
+                          method="adi", mib=2, dt=2.0 / (n - 1), setup="device")
             res = {}
-            for prec in ("plain", "mixed"):
+            for prec in ("plain", "fast", "mixed"):
                 with M.Solver(spec) as s:
                     s.set_precision(prec)
                     if prec == "plain":
@@ -149,18 +150,22 @@ def run_precision(grids=(257, 385), betas=(1e-3, 1.0, 1e3), steps: int = 20) -> 
                     ms = e0.elapsed_time(e1)
                     lmax, l2, _ = s.norms()
                     res[prec] = (ms, lmax, l2, s.solution())
-            up, um = res["plain"][3], res["mixed"][3]
+            up, uf, um = res["plain"][3], res["fast"][3], res["mixed"][3]
             nodes = n ** 3
             out[f"{n}^3 beta {b:g}"] = {
                 "plain_cell_steps_per_s": nodes * steps / (res["plain"][0] / 1e3),
+                "fast_cell_steps_per_s": nodes * steps / (res["fast"][0] / 1e3),
                 "mixed_cell_steps_per_s": nodes * steps / (res["mixed"][0] / 1e3),
                 "speedup": res["plain"][0] / res["mixed"][0],
+                "speedup_vs_fast": res["fast"][0] / res["mixed"][0],
+                "fast_speedup": res["plain"][0] / res["fast"][0],
+                "fast_rel_maxdiff": float(np.abs(uf - up).max() / np.abs(up).max()),
                 "linf_exact_plain": res["plain"][1], "linf_exact_mixed": res["mixed"][1],
                 "linf_ratio": res["mixed"][1] / res["plain"][1],
                 "linf_vs_plain_fp64": float(np.abs(um - up).max()),
                 "rel_maxdiff_vs_plain": float(np.abs(um - up).max() / np.abs(up).max()),
             }
-            del up, um, res
+            del up, uf, um, res
     return {"workload": "precision form: 257^3 and 385^3 Douglas-ADI MIB-L2 torus, beta 1e-3/1/1e3, dt = h, "
                         f"{steps} steps", "steps": steps, "cases": out}
 
@@ -211,9 +216,46 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
     M.batch_advance(solvers, steps)
     bat = time.perf_counter() - t0
     same = all(s.norms() == r for s, r in zip(solvers, ref))
+    # the same mix with its Douglas-ADI problems in the mixed form (FP32
+    # segmented line solves inside the multi-problem launches; the other
+    # methods have no mixed form and stay plain): alone, then batched
+    adi = [i for i, sp in enumerate(specs) if sp.method == "adi"]
+    for i in adi:
+        solvers[i].set_precision("mixed")
+    for s in solvers:
+        s.time = 0.0
+        s.initialize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.advance(steps)
+        s.synchronize()
+    seq_m = time.perf_counter() - t0
+    ref_m = [s.norms() for s in solvers]
+    for s in solvers:
+        s.time = 0.0
+        s.initialize()
+    M.batch_advance(solvers, 1)
+    for s in solvers:
+        s.time = 0.0
+        s.initialize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    M.batch_advance(solvers, steps)
+    bat_m = time.perf_counter() - t0
+    same_m = all(s.norms() == r for s, r in zip(solvers, ref_m))
+    ratios = [ref_m[i][0] / ref[i][0] for i in adi if ref[i][0] > 0]
+    mixed = {
+        "adi_problems_mixed": len(adi), "batched_solves_per_s": count / bat_m, "speedup": seq / bat_m,
+        "batched_cell_steps_per_s": nodes * steps / bat_m, "sequential_same_forms_s": seq_m, "batched_s": bat_m,
+        "results_identical_alone_vs_batched": same_m, "linf_ratio_max": max(ratios) if ratios else None,
+        "linf_ratio_min": min(ratios) if ratios else None,
+        "speedup_basis": "sequential plain FP64 solves of the same 512 problems",
+    }
     for s in solvers:
         s.close()
     return {
+        "mixed_adi": mixed,
         "problems": count, "steps": steps, "seed": seed, "nodes_total": nodes,
         "sequential_solves_per_s": count / seq, "batched_solves_per_s": count / bat,
         "speedup": seq / bat, "batched_cell_steps_per_s": nodes * steps / bat,
@@ -728,6 +770,9 @@ def main():
         line["exact_plain"] = exact
     if mixed is not None:
         line["mixed"] = mixed
+    if rank == 0 and world == 1 and not a.no_mixed and w["method"] == "adi":
+        # the precision form's second grid of its config, 385^3, one beta ratio
+        line["precision_385"] = run_precision(grids=(385,), betas=(1e3,), steps=10)
     if rank == 0 and world == 1 and not a.no_batched:
         line["batched"] = run_batched(a.batch_problems, a.batch_steps)
     if rank == 0 and world == 1 and not a.no_served:

@@ -499,6 +499,7 @@ mts_status finish_create(mts_problem* h) {
     mts::configure_mixed_kernels();
     mts::configure_batch_kernels();
     mts::configure_fast_kernels();
+    mts::configure_mixed_batch_kernels();
     configured = true;
   }
   int sms = 0;
@@ -993,12 +994,22 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     for (int d = 1; d < 3; d++) lines = std::min(lines, (long long)line_count(h->g, d));
     return lines >= 256LL * h->dev.sweep_blocks;
   };
-  auto solo = [&](int i) { return hs[i]->dev.precision != 0 || fills_gpu(hs[i]); };
+  // mixed-form ADI problems whose lines fit the batched segmented solves
+  // (at most 160 rows) batch in a group of their own
+  auto mixed_batchable = [&](const mts_problem* h) {
+    if (h->dev.precision != 1 || h->prm.method != MTS_ADI) return false;
+    for (int d = 0; d < 3; d++)
+      if (mts::mixed_batch_class(h->dev, d) < 0) return false;
+    return true;
+  };
+  auto solo = [&](int i) {
+    return fills_gpu(hs[i]) || (hs[i]->dev.precision != 0 && !mixed_batchable(hs[i]));
+  };
   // plain handles by method: one batched launch sequence per group
   for (int method = 0; method < 4; method++) {
     std::vector<int> mem;
     for (int i = 0; i < n; i++)
-      if (!solo(i) && hs[i]->prm.method == method) mem.push_back(i);
+      if (!solo(i) && hs[i]->dev.precision == 0 && hs[i]->prm.method == method) mem.push_back(i);
     if (mem.empty()) continue;
     cudaStream_t q = nullptr;
     BATCH_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
@@ -1048,6 +1059,59 @@ mts_status mts_batch_advance_steps(const mts_handle* hs, const int32_t* counts, 
     for (int k = 0; k < gsteps; k++) launches += mts::launch_step_batch(plan, q);
     BATCH_TRY(cudaGetLastError());
     for (int i : mem) hs[i]->launches += launches;
+  }
+  // the mixed-form group: one batched launch sequence of the mixed step
+  {
+    std::vector<int> mem;
+    for (int i = 0; i < n; i++)
+      if (!solo(i) && hs[i]->dev.precision == 1) mem.push_back(i);
+    if (!mem.empty()) {
+      cudaStream_t q = nullptr;
+      BATCH_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+      streams.push_back(q);
+      std::vector<mts::Dev> recs;
+      mts::MixedBatchPlan plan{};
+      plan.n = (int)mem.size();
+      std::vector<mts::BatchItem> jumps, rows, mib, blk[3], line[3][2];
+      auto add = [](std::vector<mts::BatchItem>& v, int p, unsigned ncta) {
+        for (unsigned c = 0; c < ncta; c++) v.push_back(mts::BatchItem{p, (int32_t)c, (int32_t)ncta, 0});
+      };
+      for (int k = 0; k < (int)mem.size(); k++) {
+        const mts::Dev& d = hs[mem[(size_t)k]]->dev;
+        recs.push_back(d);
+        if (d.ncross > 0) add(jumps, k, mts::jumps_grid(d));
+        add(rows, k, mts::pointwise_rows_grid(d));
+        if (d.nmibnode > 0) add(mib, k, mts::mib_grid(d));
+        for (int dd = 0; dd < 3; dd++) {
+          if (d.nblk[dd] > 0) add(blk[dd], k, mts::block_grid(d, dd));
+          add(line[dd][mts::mixed_batch_class(d, dd)], k, mts::mixed_line_ctas(d, dd));
+        }
+      }
+      void* tmp = nullptr;
+      BATCH_TRY(dev_upload(recs.data(), recs.size() * sizeof(mts::Dev), q, &tmp));
+      plan.Ps = (const mts::Dev*)tmp;
+      auto up = [&](std::vector<mts::BatchItem>& v, const mts::BatchItem** dst, int* cnt) -> cudaError_t {
+        *cnt = (int)v.size();
+        void* p = nullptr;
+        cudaError_t e = dev_upload(v.data(), v.size() * sizeof(mts::BatchItem), q, &p);
+        *dst = (const mts::BatchItem*)p;
+        return e;
+      };
+      BATCH_TRY(up(jumps, &plan.jumps, &plan.njumps));
+      BATCH_TRY(up(rows, &plan.rows, &plan.nrows));
+      BATCH_TRY(up(mib, &plan.mib, &plan.nmib));
+      for (int dd = 0; dd < 3; dd++) {
+        BATCH_TRY(up(blk[dd], &plan.blk[dd], &plan.nblk[dd]));
+        for (int c = 0; c < 2; c++) BATCH_TRY(up(line[dd][c], &plan.line[dd][c], &plan.nline[dd][c]));
+      }
+      BATCH_TRY(cudaStreamSynchronize(q));  // the host vectors must outlive the uploads
+      int gsteps = 0;
+      for (int i : mem) gsteps = std::max(gsteps, counts[i]);
+      int64_t launches = 0;
+      for (int k = 0; k < gsteps; k++) launches += mts::launch_step_batch_mixed(plan, q);
+      BATCH_TRY(cudaGetLastError());
+      for (int i : mem) hs[i]->launches += launches;
+    }
   }
   // solo problems: their own steps on their own streams
   for (int i = 0; i < n; i++) {

@@ -223,6 +223,29 @@ struct BatchPlan {
   const BatchItem* sw[3];   // line sweeps per direction
   int nsw[3];
 };
+// The mixed form's batched step (ADI, lines of at most 160 rows): the
+// mixed kernels' bodies, one item per CTA (mixed.cu).  line[d][c]: the line
+// solves of direction d for the problems of rows-per-lane class c (3, 5).
+struct MixedBatchPlan {
+  int n;
+  const Dev* Ps;
+  const BatchItem* jumps;
+  int njumps;
+  const BatchItem* rows;
+  int nrows;
+  const BatchItem* mib;
+  int nmib;
+  const BatchItem* blk[3];
+  int nblk[3];
+  const BatchItem* line[3][2];
+  int nline[3][2];
+};
+int mixed_batch_class(const Dev& P, int d);          // -1: not batchable
+unsigned mixed_line_ctas(const Dev& P, int d);      // CTAs of the line solves of direction d
+int launch_step_batch_mixed(const MixedBatchPlan& plan, cudaStream_t stream);  // one step + tick
+void configure_mixed_batch_kernels();
+int launch_batch_jumps(const Dev* Ps, const BatchItem* items, int nitems, cudaStream_t stream);
+int launch_batch_tick(const Dev* Ps, int n, cudaStream_t stream);
 int batch_sweep_threads();                 // threads per CTA of the batched sweeps
 void configure_batch_kernels();
 int launch_step_batch(const BatchPlan& plan, cudaStream_t stream);  // one step + tick

@@ -298,5 +298,19 @@ struct IntC {
   static constexpr int value = I;
 };
 
+// The CTA's item and its problem's record, copied into shared memory.
+#define BATCH_PROLOGUE                                                                \
+  __shared__ __align__(16) long long sdev_[(sizeof(Dev) + 7) / 8];                    \
+  const BatchItem w = items[blockIdx.x];                                              \
+  {                                                                                   \
+    const long long* src_ = reinterpret_cast<const long long*>(Ps + w.p);             \
+    for (int i_ = threadIdx.x; i_ < (int)((sizeof(Dev) + 7) / 8); i_ += blockDim.x) \
+      sdev_[i_] = src_[i_];                                                           \
+  }                                                                                   \
+  __syncthreads();                                                                    \
+  const Dev& P = *reinterpret_cast<const Dev*>(sdev_);                                \
+  if (*P.tstep >= P.tstop) return; /* this problem's steps of the batch are done */
+
+
 }  // namespace
 }  // namespace mts

@@ -1372,19 +1372,6 @@ __device__ __forceinline__ SweepIO make_io(const Dev& P, const Roles& r) {
   return io;
 }
 
-// The CTA's item and its problem's record, copied into shared memory.
-#define BATCH_PROLOGUE                                                                \
-  __shared__ __align__(16) long long sdev_[(sizeof(Dev) + 7) / 8];                    \
-  const BatchItem w = items[blockIdx.x];                                              \
-  {                                                                                   \
-    const long long* src_ = reinterpret_cast<const long long*>(Ps + w.p);             \
-    for (int i_ = threadIdx.x; i_ < (int)((sizeof(Dev) + 7) / 8); i_ += blockDim.x) \
-      sdev_[i_] = src_[i_];                                                           \
-  }                                                                                   \
-  __syncthreads();                                                                    \
-  const Dev& P = *reinterpret_cast<const Dev*>(sdev_);                                \
-  if (*P.tstep >= P.tstop) return; /* this problem's steps of the batch are done */
-
 __global__ void __launch_bounds__(TPB) kb_jumps(const Dev* __restrict__ Ps, const BatchItem* __restrict__ items) {
   BATCH_PROLOGUE
   k_jumps_body(P, w.cta, w.ncta, 0.0);
@@ -1458,6 +1445,17 @@ void bsweep_attr() {
 }  // namespace
 
 int batch_sweep_threads() { return BNT; }
+
+int launch_batch_jumps(const Dev* Ps, const BatchItem* items, int nitems, cudaStream_t st) {
+  if (nitems <= 0) return 0;
+  kb_jumps<<<nitems, TPB, 0, st>>>(Ps, items);
+  return 1;
+}
+
+int launch_batch_tick(const Dev* Ps, int n, cudaStream_t st) {
+  kb_tick<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(Ps, n);
+  return 1;
+}
 
 unsigned jumps_grid(const Dev& P) { return (unsigned)((P.ncross + TPB - 1) / TPB); }
 unsigned mib_grid(const Dev& P) { return (unsigned)((P.nmibnode + TPB - 1) / TPB); }

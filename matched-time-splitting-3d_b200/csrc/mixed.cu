@@ -29,8 +29,8 @@ namespace {
 // Residual rho = dt (A_x u + A_y u + A_z u + src), FP64 in, FP32 out.
 
 template <int G>
-__global__ void __launch_bounds__(TPB, 8) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                   float* __restrict__ rho, double E) {
+__device__ __forceinline__ void adi_resid_body(const Dev& P, unsigned cta_, unsigned ncta_,
+                                               const double* __restrict__ un, float* __restrict__ rho, double E) {
   E = step_e(P, E, 2);
   const long long sy = P.nx, sz = (long long)P.nx * P.ny;
   const int lane = threadIdx.x & 31;
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(TPB, 8) k_adi_resid(const __grid_constant__ De
   // a node's side selects one of two specialised bodies (uniform over a
   // warp away from the interface), whose stencil weights are fixed kernel
   // parameters (constant-bank operands, no registers)
-  for (int row = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += gridDim.x * (TPB / 32)) {
+  for (int row = cta_ * (TPB / 32) + (threadIdx.x >> 5); row < nrows; row += ncta_ * (TPB / 32)) {
     const int iy = row % P.ny, iz = row / P.ny;
     const long long m0 = (long long)P.nx * row;
     const RowExact q = row_exact(P, iy, iz);
@@ -98,12 +98,18 @@ __global__ void __launch_bounds__(TPB, 8) k_adi_resid(const __grid_constant__ De
   }
 }
 
+template <int G>
+__global__ void __launch_bounds__(TPB, 8) k_adi_resid(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                   float* __restrict__ rho, double E) {
+  adi_resid_body<G>(P, blockIdx.x, gridDim.x, un, rho, E);
+}
+
 // The MIB rows of rho, one thread per listed node: the explicit MIB sums of
 // every direction the node is a MIB row of (douglas_adi.cc:112-210, without
 // jumps) and the jump terms of Src_2nd (douglas_adi.cc:1156-1427).
-__global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
-                                                       float* __restrict__ rho, double E) {
-  const int k = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void adi_resid_mib_body(const Dev& P, unsigned cta_, const double* __restrict__ un,
+                                                   float* __restrict__ rho, double E) {
+  const int k = cta_ * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   E = step_e(P, E, 2);
   const long long m = P.mibnode[k];
@@ -145,6 +151,11 @@ __global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ D
   rho[m] = (float)(P.dt * (((sx + sy_) + sz_) + src));
 }
 
+__global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
+                                                       float* __restrict__ rho, double E) {
+  adi_resid_mib_body(P, blockIdx.x, un, rho, E);
+}
+
 // ---------------------------------------------------------------------------
 // FP32 line solves of the increments.
 
@@ -153,9 +164,8 @@ __global__ void __launch_bounds__(TPB) k_adi_resid_mib(const __grid_constant__ D
 // INPLACE (the segmented solves): the results replace the rows' right-hand
 // sides in the field, else they go to rblk32 for the ring sweeps.
 template <int D, bool INPLACE>
-__global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev P, float* __restrict__ f,
-                                                     int nblk) {
-  const int k = blockIdx.x * TPB + threadIdx.x;
+__device__ __forceinline__ void block_rhs32_body(const Dev& P, unsigned cta_, float* __restrict__ f, int nblk) {
+  const int k = cta_ * TPB + threadIdx.x;
   if (k >= nblk) return;
   const MibBlock& b = P.blk[D][k];
   const int n2 = D == 2 ? P.ny : P.nz;
@@ -178,6 +188,12 @@ __global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev
     for (int q = 0; q < b.kind; q++) f[L.base + (long long)(b.L + q) * L.s] = (float)r[q];
   else
     for (int q = 0; q < 3; q++) P.rblk32[D][3 * k + q] = (float)r[q];
+}
+
+template <int D, bool INPLACE>
+__global__ void __launch_bounds__(TPB) k_block_rhs32(const __grid_constant__ Dev P, float* __restrict__ f,
+                                                     int nblk) {
+  block_rhs32_body<D, INPLACE>(P, blockIdx.x, f, nblk);
 }
 
 struct BlockHead32 {
@@ -635,7 +651,7 @@ __device__ __forceinline__ void load_row_tables(float* tab, const float* ctab, i
 
 // x lines: contiguous in memory, so a warp copies its own line in and out.
 template <int MX>
-__global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant__ Dev P, float* __restrict__ f) {
+__device__ __forceinline__ void xline32_body(const Dev& P, unsigned cta_, unsigned ncta_, float* __restrict__ f) {
   static_assert(MX & 1, "odd rows per lane");
   constexpr int R = 32 * MX;
   constexpr int LS = 4 * R + 4;
@@ -650,7 +666,7 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant
   const float* __restrict__ cib = P.cib[0];
   const float* __restrict__ cpp = P.cp[0];
   const float* __restrict__ cqq = P.cq[0];
-  for (long long t = (long long)blockIdx.x * WL_WARPS + w; t < nl; t += (long long)gridDim.x * WL_WARPS) {
+  for (long long t = (long long)cta_ * WL_WARPS + w; t < nl; t += (long long)ncta_ * WL_WARPS) {
     Line L;
     decode_line<0>(P, t, L);
     if (L.boundary) continue;  // face line: its right-hand side is its solution (warp-uniform)
@@ -682,6 +698,11 @@ __global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant
       if (j < n) f[L.base + j] = sr[j];
     }
   }
+}
+
+template <int MX>
+__global__ void __launch_bounds__(32 * WL_WARPS) k_xline32(const __grid_constant__ Dev P, float* __restrict__ f) {
+  xline32_body<MX>(P, blockIdx.x, gridDim.x, f);
 }
 
 // y and z lines: strided, so the CTA copies NL neighbouring lines together,
@@ -716,8 +737,8 @@ constexpr size_t yzline_smem() {
 }
 
 template <int D, int MX, bool ACC>
-__global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
-                                                          double* __restrict__ u) {
+__device__ __forceinline__ void yzline32_body(const Dev& P, unsigned cta_, unsigned ncta_, float* __restrict__ f,
+                                              double* __restrict__ u) {
   static_assert(MX & 1, "odd rows per lane");
   static_assert(D != 0 && (!ACC || D == 2), "y and z lines; accumulation after the z solve");
   constexpr int R = 32 * MX;
@@ -735,7 +756,7 @@ __global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __g
   // this thread's share of a copy: line c, rows jc + 32 m
   const int c = threadIdx.x & (NL - 1), jc = threadIdx.x / NL;
   const long long nl = nlines<D>(P);
-  const long long stride = (long long)gridDim.x * NL;
+  const long long stride = (long long)ncta_ * NL;
   const float* __restrict__ cib = P.cib[D];
   const float* __restrict__ cpp = P.cp[D];
   const float* __restrict__ cqq = P.cq[D];
@@ -778,7 +799,7 @@ __global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __g
     return cp;
   };
 
-  for (long long t0 = (long long)blockIdx.x * NL; t0 < nl; t0 += stride) {
+  for (long long t0 = (long long)cta_ * NL; t0 < nl; t0 += stride) {
     // a thread copies into exactly the rows it stored from last time: no
     // barrier needed before the copy
     const Copy cur = copy_in(t0);
@@ -814,6 +835,12 @@ __global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __g
       }
     }
   }
+}
+
+template <int D, int MX, bool ACC>
+__global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) k_yzline32(const __grid_constant__ Dev P, float* __restrict__ f,
+                                                          double* __restrict__ u) {
+  yzline32_body<D, MX, ACC>(P, blockIdx.x, gridDim.x, f, u);
 }
 
 // u^{n+1} = u^n + d, four nodes per thread
@@ -879,6 +906,72 @@ void launch_wline_n(const Dev& P, float* f, double* u, cudaStream_t st) {
     launch_wline<D, 17>(P, f, u, st);
 }
 
+// ---------------------------------------------------------------------------
+// The mixed step inside multi-problem launches: one item per CTA (its
+// problem, its CTA index in that problem's own launch, that launch's CTA
+// count); the CTA runs the same body as the problem's own launch, so a
+// problem computes the same bits alone or in a batch.  The step's time
+// factors come from the step table (step_e).
+
+__global__ void __launch_bounds__(TPB, 8) kbm_adi_resid(const Dev* __restrict__ Ps,
+                                                        const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  adi_resid_body<2>(P, w.cta, w.ncta, P.u0, P.r32, 0.0);
+}
+
+__global__ void __launch_bounds__(TPB) kbm_adi_resid_mib(const Dev* __restrict__ Ps,
+                                                         const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  adi_resid_mib_body(P, w.cta, P.u0, P.r32, 0.0);
+}
+
+template <int D>
+__global__ void __launch_bounds__(TPB) kbm_block_rhs32(const Dev* __restrict__ Ps,
+                                                       const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  block_rhs32_body<D, true>(P, w.cta, P.r32, P.nblk[D]);
+}
+
+template <int MX>
+__global__ void __launch_bounds__(32 * WL_WARPS) kbm_xline32(const Dev* __restrict__ Ps,
+                                                             const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  xline32_body<MX>(P, w.cta, w.ncta, P.r32);
+}
+
+template <int D, int MX, bool ACC>
+__global__ void __launch_bounds__(32 * yz_lines<ACC, MX>()) kbm_yzline32(const Dev* __restrict__ Ps,
+                                                                      const BatchItem* __restrict__ items) {
+  BATCH_PROLOGUE
+  yzline32_body<D, MX, ACC>(P, w.cta, w.ncta, P.r32, ACC ? P.u0 : nullptr);
+}
+
+// rows per lane of the batched classes
+constexpr int kBatchMX[2] = {3, 5};
+
+template <int D, int MX>
+void launch_batch_lines(const BatchItem* items, int n, const Dev* Ps, cudaStream_t st) {
+  if (n <= 0) return;
+  if (D == 0)
+    kbm_xline32<MX><<<n, 32 * WL_WARPS, xline_smem<MX>(), st>>>(Ps, items);
+  else if (D == 1)
+    kbm_yzline32<1, MX, false><<<n, 32 * yz_lines<false, MX>(), yzline_smem<MX, false>(), st>>>(Ps, items);
+  else
+    kbm_yzline32<2, MX, true><<<n, 32 * yz_lines<true, MX>(), yzline_smem<MX, true>(), st>>>(Ps, items);
+}
+
+template <int D>
+int launch_batch_dir(const MixedBatchPlan& b, cudaStream_t st) {
+  int launches = 0;
+  if (b.nblk[D] > 0) {
+    kbm_block_rhs32<D><<<b.nblk[D], TPB, 0, st>>>(b.Ps, b.blk[D]);
+    launches++;
+  }
+  launch_batch_lines<D, kBatchMX[0]>(b.line[D][0], b.nline[D][0], b.Ps, st);
+  launch_batch_lines<D, kBatchMX[1]>(b.line[D][1], b.nline[D][1], b.Ps, st);
+  return launches + (b.nline[D][0] > 0) + (b.nline[D][1] > 0);
+}
+
 template <int D>
 void sweep32(const Dev& P, float* f, double* u, cudaStream_t st) {
   const int nd = D == 0 ? P.nx : D == 1 ? P.ny : P.nz;
@@ -940,6 +1033,50 @@ int build_mixed_coefs(const Dev& P, cudaStream_t st) {
   k_ctab32<1><<<(2 * P.ny + TPB - 1) / TPB, TPB, 0, st>>>(P);
   k_ctab32<2><<<(2 * P.nz + TPB - 1) / TPB, TPB, 0, st>>>(P);
   return 6;
+}
+
+int mixed_batch_class(const Dev& P, int d) {
+  if (!P.cib[0] || !P.cib[1] || !P.cib[2]) return -1;  // no segmented coefficients
+  const int nd = d == 0 ? P.nx : d == 1 ? P.ny : P.nz;
+  for (int c = 0; c < 2; c++)
+    if (nd <= 32 * kBatchMX[c]) return c;
+  return -1;
+}
+
+unsigned mixed_line_ctas(const Dev& P, int d) {
+  const int c = mixed_batch_class(P, d);
+  const int mx = c >= 0 ? kBatchMX[c] : kBatchMX[1];
+  if (d == 0) return (unsigned)((nlines<0>(P) + WL_WARPS - 1) / WL_WARPS);
+  const int nl = d == 2 ? (mx == 3 ? yz_lines<true, 3>() : yz_lines<true, 5>())
+                        : (mx == 3 ? yz_lines<false, 3>() : yz_lines<false, 5>());
+  return (unsigned)(((d == 1 ? nlines<1>(P) : nlines<2>(P)) + nl - 1) / nl);
+}
+
+void configure_mixed_batch_kernels() {
+  cudaFuncSetAttribute(kbm_xline32<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xline_smem<3>());
+  cudaFuncSetAttribute(kbm_xline32<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xline_smem<5>());
+  cudaFuncSetAttribute(kbm_yzline32<1, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<3, false>());
+  cudaFuncSetAttribute(kbm_yzline32<1, 5, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<5, false>());
+  cudaFuncSetAttribute(kbm_yzline32<2, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<3, true>());
+  cudaFuncSetAttribute(kbm_yzline32<2, 5, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)yzline_smem<5, true>());
+}
+
+int launch_step_batch_mixed(const MixedBatchPlan& b, cudaStream_t st) {
+  int launches = launch_batch_jumps(b.Ps, b.jumps, b.njumps, st);
+  if (b.nmib > 0) {
+    kbm_adi_resid_mib<<<b.nmib, TPB, 0, st>>>(b.Ps, b.mib);
+    launches++;
+  }
+  kbm_adi_resid<<<b.nrows, TPB, 0, st>>>(b.Ps, b.rows);
+  launches++;
+  launches += launch_batch_dir<0>(b, st);
+  launches += launch_batch_dir<1>(b, st);
+  launches += launch_batch_dir<2>(b, st);
+  return launches + launch_batch_tick(b.Ps, b.n, st);
 }
 
 int launch_step_mixed(const Dev& P, const StepTimes& T, double* u, cudaStream_t st, cudaEvent_t* ev,

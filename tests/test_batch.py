@@ -116,3 +116,38 @@ def test_batch_with_large_problems_on_their_own_streams():
     finally:
         for s in solvers:
             s.close()
+
+
+def test_mixed_problems_batch_in_their_own_group():
+    """Mixed-precision Douglas-ADI problems with lines of at most 160 rows
+    advance together in one batched launch sequence of the mixed step (the
+    FP32 segmented solves, a warp per line, inside multi-problem launches):
+    bit-identical to stepping each alone, beside plain problems of every
+    method, with uneven step counts; their L-infinity error stays within
+    1.05x of the plain form's."""
+    rng = np.random.default_rng(21)
+    specs = []
+    while len([s for s in specs if s.method == "adi"]) < 6:
+        specs.append(draw(rng, sizes=(17, 25, 33, 49, 65)))
+    precision = ["mixed" if s.method == "adi" else "plain" for s in specs]
+    counts = [4 + (i % 5) for i in range(len(specs))]
+    solvers = [M.Solver(sp) for sp in specs]
+    try:
+        for s, p in zip(solvers, precision):
+            s.set_precision(p)
+            s.initialize()
+        M.batch_advance_steps(solvers, counts)
+        for sp, s, p, k in zip(specs, solvers, precision, counts):
+            u, t = solve_alone(sp, p, k)
+            assert s.time == t
+            assert np.array_equal(s.solution(), u), (sp, p)
+            if p == "mixed":
+                with M.Solver(sp) as ref:
+                    ref.initialize()
+                    ref.advance(k)
+                    ref.synchronize()
+                    lp = ref.norms()[0]
+                assert s.norms()[0] <= 1.05 * lp + 1e-12, (sp, s.norms()[0], lp)
+    finally:
+        for s in solvers:
+            s.close()
