@@ -287,7 +287,10 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
             q.spec = dataclasses.replace(q.spec, setup="device")
         return reqs
 
-    out = {"requests_per_rate": count, "hbm_budget_bytes": budget, "setup": "device", "rates": {}}
+    out = {"requests_per_rate": count, "hbm_budget_bytes": budget, "setup": "device",
+           "server_forms": "Douglas-ADI requests in the mixed form (FP32 segmented solves, batched), the others "
+                           "plain FP64; the sequential arm solves every request in plain FP64",
+           "rates": {}}
     t_gen = time.perf_counter()
     stream = on_device(served_requests(count, 1000.0, seed, validate=setup_device))
     out["stream_generation_s"] = time.perf_counter() - t_gen
@@ -299,13 +302,16 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
     rs = np.random.default_rng(seed + 1)
     svc = {}
     serve.solve_alone(stream[0])  # module loading and first-launch costs, not timed
+    plain_lmax = {}  # request id -> L-infinity error of its plain solve (the sample's Douglas-ADI requests)
     for c, v in classes.items():
         pick = rs.choice(len(v), min(per_class.get(c, 8), len(v)), replace=False)
         times = []
         for i in pick:
             t0 = time.perf_counter()
-            serve.solve_alone(v[int(i)])
+            r = serve.solve_alone(v[int(i)])
             times.append(time.perf_counter() - t0)
+            if v[int(i)].spec.method == "adi":
+                plain_lmax[r.id] = r.lmax
         svc[c] = np.array(times)
     mean_svc = sum(share[c] * svc[c].mean() for c in svc)
     out["sequential_solves_per_s"] = float(1.0 / mean_svc)
@@ -314,10 +320,11 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
     rng = np.random.default_rng(seed + 2)
     for rate in rates:
         reqs = on_device(served_requests(count, rate, seed, validate=setup_device))
-        srv = serve.Server(hbm_budget=budget, setup="device")
+        srv = serve.Server(hbm_budget=budget, setup="device", precision="mixed")
         t0 = time.perf_counter()
         res = srv.run(reqs)
         span = time.perf_counter() - t0
+        ratios = [r.lmax / plain_lmax[r.id] for r in res if r.id in plain_lmax and plain_lmax[r.id] > 0]
         lat = np.array([r.latency for r in res])
         arr = np.array([q.arrival for q in reqs])
         seq_svc = np.array([rng.choice(svc[size_class(q.spec)]) for q in reqs])
@@ -329,6 +336,7 @@ def run_served(count: int, rates: list[float], seed: int = 0, budget: float = 12
             "peak_budget_bytes": srv.peak_bytes, "batches": srv.batches,
             "loop_batch_s": srv.batch_s, "loop_retire_s": srv.retire_s,
             "solves_per_s_vs_sequential": len(res) / span / out["sequential_solves_per_s"],
+            "adi_linf_ratio_vs_plain_max": max(ratios) if ratios else None, "adi_linf_ratio_samples": len(ratios),
         }
     out["timing"] = ("wall clock from the first arrival to the last completion; latency = completion - arrival; "
                      "sequential: service times measured per grid class on a stratified sample, latencies from a "
