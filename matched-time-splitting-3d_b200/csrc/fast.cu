@@ -448,41 +448,39 @@ __device__ __forceinline__ void load_tab(double* s, const double* g, int w2) {
 
 __global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
                                               double* __restrict__ d, double E) {
-  const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
-  E = step_e(P, E, 2);
-  const int nxb = P.nblk[0];
-  if (t < nxb) {
-    // an x block: rho of its rows, then the Convert2Tri row operations
-    const MibBlock& b = P.blk[0][t];
-    const int iy = b.line / P.nz, iz = b.line % P.nz;
-    const long long m0 = (long long)P.nx * (iy + (long long)P.ny * iz);
-    double r[3] = {0.0, 0.0, 0.0};
-    for (int q = 0; q < b.kind; q++) {
-      const long long m = m0 + b.L + q;
-      r[q] = rho_mib(P, un, E, m, b.L + q, iy, iz, P.tag[m], P.mibref[P.xbmib[3 * t + q]]);
-    }
-    if (b.kind == 2) {
-      r[1] -= b.rate[0] * r[0];
-      r[0] -= b.rate[1] * r[1];
-    } else {
-      r[1] -= b.rate[0] * r[0];
-      r[2] -= b.rate[1] * r[0];
-      r[0] -= b.rate[2] * r[2];
-      r[1] -= b.rate[3] * r[2];
-      r[2] -= b.rate[4] * r[1];
-      r[0] -= b.rate[5] * r[1];
-    }
-    for (int q = 0; q < b.kind; q++) d[m0 + b.L + q] = r[q];
-    return;
-  }
-  const long long k = t - nxb;
+  // every MIB row at once, one thread each (the rows of an x block too:
+  // kf_mib_xblk then applies their block's row operations)
+  const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
-  const int4 ref = P.mibref[k];
-  if (ref.x >= 0) return;  // its x block's thread writes it
+  E = step_e(P, E, 2);
   const long long m = P.mibnode[k];
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
-  d[m] = rho_mib(P, un, E, m, ix, iy, iz, P.tag[m], ref);
+  d[m] = rho_mib(P, un, E, m, ix, iy, iz, P.tag[m], P.mibref[k]);
+}
+
+// The Convert2Tri row operations of the x blocks (douglas_adi.cc:1554-1675)
+// on the rows' right-hand sides that kf_mib wrote, one thread per block.
+__global__ void __launch_bounds__(TPB) kf_mib_xblk(const __grid_constant__ Dev P, double* __restrict__ d) {
+  const int t = blockIdx.x * TPB + threadIdx.x;
+  if (t >= P.nblk[0]) return;
+  const MibBlock& b = P.blk[0][t];
+  const int iy = b.line / P.nz, iz = b.line % P.nz;
+  const long long m0 = (long long)P.nx * (iy + (long long)P.ny * iz) + b.L;
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < b.kind; q++) r[q] = d[m0 + q];
+  if (b.kind == 2) {
+    r[1] -= b.rate[0] * r[0];
+    r[0] -= b.rate[1] * r[1];
+  } else {
+    r[1] -= b.rate[0] * r[0];
+    r[2] -= b.rate[1] * r[0];
+    r[0] -= b.rate[2] * r[2];
+    r[1] -= b.rate[3] * r[2];
+    r[2] -= b.rate[4] * r[1];
+    r[0] -= b.rate[5] * r[1];
+  }
+  for (int q = 0; q < b.kind; q++) d[m0 + q] = r[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -1430,9 +1428,12 @@ int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cud
     launches += cross ? 2 : 1;
   };
   mark(0);
-  if (P.nblk[0] > 0 || P.nmibnode > 0) {
-    const long long nt = (long long)P.nblk[0] + P.nmibnode;
-    kf_mib<<<(unsigned)((nt + TPB - 1) / TPB), TPB, 0, st>>>(P, u, d, T.e_next);
+  if (P.nmibnode > 0) {
+    kf_mib<<<(unsigned)((P.nmibnode + TPB - 1) / TPB), TPB, 0, st>>>(P, u, d, T.e_next);
+    launches++;
+  }
+  if (P.nblk[0] > 0) {
+    kf_mib_xblk<<<(unsigned)((P.nblk[0] + TPB - 1) / TPB), TPB, 0, st>>>(P, d);
     launches++;
   }
   pass(0, u, d, nullptr, T.e_next);

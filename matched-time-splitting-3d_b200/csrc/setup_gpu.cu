@@ -533,7 +533,7 @@ struct SetupArgs {
   int mib;
 };
 
-constexpr int kCtrlTagErr = 0, kCtrlCorners = 1, kCtrlListed = 2, kCtrlFirstBad = 3, kCtrlStatus = 4;
+constexpr int kCtrlTagErr = 0, kCtrlCorners = 1, kCtrlListed = 2, kCtrlFirstBad = 3;
 constexpr int kCtrlInts = 8;
 
 __global__ void k_su_tags(const SetupArgs A) {
