@@ -73,7 +73,7 @@ class Server:
       threads) or "device" (the same on the GPU, mts_setup_device)."""
 
     def __init__(self, hbm_budget: float = 120e9, chunk_steps: int = 32, host_threads: int = 16,
-                 keep_solutions: bool = False, precision: str = "plain", max_active: int = 256,
+                 keep_solutions: bool = False, precision: str = "plain", max_active: int = 384,
                  setup: str = "host"):
         self.budget = int(hbm_budget)
         self.max_active = max(1, int(max_active))
