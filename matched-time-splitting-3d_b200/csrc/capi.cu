@@ -79,6 +79,10 @@ struct mts_problem {
   double* norm_part = nullptr;
   double* norm_out = nullptr;
   mts::SideStream side{nullptr, nullptr, nullptr};  // the mixed form's second stream
+  // the fast and mixed forms' data are built on the first switch to the
+  // form; a build that fails part way is done again on the next switch
+  bool fast_built = false;
+  bool mixed_built = false;
   // the fictitious points' error report (mts_fp_errors), built on first use
   mts_crossing* fp_cr = nullptr;
   int32_t* fp_ci = nullptr;
@@ -1260,10 +1264,21 @@ mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
       role[(size_t)i + 1] = 2;
       i += 2;
     }
-    CUDA_TRY(h->put(&h->fp_cr, rec.data(), rec.size()));
-    CUDA_TRY(h->put(&h->fp_ci, perm.data(), perm.size()));
-    CUDA_TRY(h->put(&h->fp_role, role.data(), role.size()));
-    CUDA_TRY(h->put(&h->fp_err, (const double*)nullptr, 2 * (size_t)n));
+    // (the handle takes the buffers only once all of them are in place, so
+    // a failed first call leaves nothing half built for the next one)
+    mts_crossing* cr = nullptr;
+    int32_t* ci = nullptr;
+    int8_t* ro = nullptr;
+    double* er = nullptr;
+    CUDA_TRY(h->put(&cr, rec.data(), rec.size()));
+    CUDA_TRY(h->put(&ci, perm.data(), perm.size()));
+    CUDA_TRY(h->put(&ro, role.data(), role.size()));
+    CUDA_TRY(h->put(&er, (const double*)nullptr, 2 * (size_t)n));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));  // the host vectors must outlive the uploads
+    h->fp_cr = cr;
+    h->fp_ci = ci;
+    h->fp_role = ro;
+    h->fp_err = er;
   }
   std::vector<double> err(2 * (size_t)n);
   if (n > 0) {
@@ -1396,7 +1411,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
     if (h->prm.method != MTS_ADI) return fail(MTS_ERR_ARG, "the fast FP64 form is built for Douglas-ADI only");
     if (!mts::fast_fits(h->g.nx, h->g.ny, h->g.nz))
       return fail(MTS_ERR_ARG, "grid lines too long for the fast FP64 form (at most 544 nodes per axis)");
-    if (!h->dev.ftab[0]) {
+    if (!h->fast_built) {
       // row tables, line flags, the crossing lines' list and coefficients,
       // the block rows' q and the MIB nodes' block references, once per
       // handle
@@ -1455,6 +1470,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
       mts::build_fast_tables(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(cudaStreamSynchronize(h->stream));
+      h->fast_built = true;
     }
   }
   if (precision == MTS_PRECISION_MIXED) {
@@ -1462,7 +1478,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
     const int nmax = std::max(h->g.nx, std::max(h->g.ny, h->g.nz));
     if (!mts::mixed_shape_fits(nmax))
       return fail(MTS_ERR_ARG, "grid lines too long for the mixed-precision sweeps' shared memory");
-    if (mts::mixed_segments_fit(nmax) && !h->dev.cib[0]) {
+    if (mts::mixed_segments_fit(nmax) && !h->mixed_built) {
       // the segmented solves' per-node coefficients, once per handle
       const size_t N = (size_t)h->g.nodes();
       const int nd[3] = {h->g.nx, h->g.ny, h->g.nz};
@@ -1479,6 +1495,7 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
       }
       mts::build_mixed_coefs(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
+      h->mixed_built = true;
     }
 
   }
