@@ -414,13 +414,19 @@ __device__ __forceinline__ void solve_tab(double* buf, const double* tab, int la
 template <int MX>
 struct LineCoef {
   double ib[MX], p[MX];
-  __device__ __forceinline__ void load(const double* __restrict__ cf, int lane) {
+  // The line's (ib, p) by row: cf, its own, from its first MIB row L1 on;
+  // before that the row table of the side of its row 1, tab (same layout),
+  // which holds the same values (the factors up to L1 are the prefix
+  // factors of that side) and stays in cache.
+  __device__ __forceinline__ void load(const double* __restrict__ cf, const double* __restrict__ tab, int L1,
+                                       int lane) {
     constexpr int R = 32 * MX;
     const int jb = lane * MX;
 #pragma unroll
     for (int k = 0; k < MX; k++) {
-      ib[k] = __ldg(cf + jb + k);
-      p[k] = __ldg(cf + R + jb + k);
+      const double* const src = jb + k < L1 ? tab : cf;
+      ib[k] = __ldg(src + jb + k);
+      p[k] = __ldg(src + R + jb + k);
     }
   }
   // p as the q of the lane's rows, before the block rows' own go over it
@@ -832,7 +838,8 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_xc(const __grid_constant__ Dev 
     const int iy = (int)(lid / nz), iz = (int)(lid % nz);
     const int bfirst = P.bstart[0][lid], bend = P.bstart[0][lid + 1];
     LineCoef<MX> cf;
-    cf.load(P.fcoef[0] + (size_t)c * 2 * R, lane);
+    cf.load(P.fcoef[0] + (size_t)c * 2 * R, P.ftab[0] + (size_t)((P.lside[0][lid] >> 1) & 1) * tabw<MX>(),
+            P.blk[0][bfirst].L, lane);
     x_rho<MX>(P, un, dst, E, iy, iz, buf, lane);
     cf.put_q(qbuf, lane);
     __syncwarp();
@@ -1038,9 +1045,10 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_yc(const __grid_constant__ Dev 
     LineCoef<MX> cf;
     int bfirst = 0, bend = 0;
     if (lw0 >= 0) {
-      cf.load(P.fcoef[D] + (size_t)(t * CW + w) * 2 * R, lane);
       bfirst = P.bstart[D][lw0];
       bend = P.bstart[D][lw0 + 1];
+      cf.load(P.fcoef[D] + (size_t)(t * CW + w) * 2 * R,
+              P.ftab[D] + (size_t)((P.lside[D][lw0] >> 1) & 1) * tabw<MX>(), P.blk[D][bfirst].L, lane);
     }
     if (ACC)
       cp_async_wait<2>();
