@@ -1459,14 +1459,8 @@ mts_status mts_set_precision(mts_handle h, int32_t precision) {
         CUDA_TRY(cudaStreamSynchronize(h->stream));
       }
       int4* ref = nullptr;
-      int32_t* xb = nullptr;
       if (D.nmibnode > 0) CUDA_TRY(h->put(&ref, (const int4*)nullptr, (size_t)D.nmibnode));
-      if (h->nblk[0] > 0) {
-        CUDA_TRY(h->put(&xb, (const int32_t*)nullptr, 3 * (size_t)h->nblk[0]));
-        CUDA_TRY(cudaMemsetAsync(xb, 0, 3 * (size_t)h->nblk[0] * sizeof(int32_t), h->stream));
-      }
       D.mibref = ref;
-      D.xbmib = xb;
       mts::build_fast_tables(h->dev, h->stream);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(cudaStreamSynchronize(h->stream));

@@ -139,7 +139,6 @@ struct Dev {
   const double* fcoef[3];
   const double* fbq[3];
   const int4* mibref;
-  const int32_t* xbmib;
   // Replayable steps (batches captured in a CUDA graph): when tsched is set,
   // kernels take the step's exp(-t) factors from tsched[3*(*tstep) + {0: t_prev,
   // 1: t_half, 2: t_next}] instead of their arguments; k_tick advances tstep.
@@ -198,7 +197,7 @@ void configure_fast_kernels();
 int fast_rows_per_lane(int n);               // MX of a direction with n rows (0: lines too long)
 bool fast_fits(int nx, int ny, int nz);      // the form takes this grid
 int build_fast_lines(const Dev& P, uint8_t* const fline[3], cudaStream_t stream);  // the line flags
-int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab, fcoef, fbq, mibref, xbmib (allocated by the caller)
+int build_fast_tables(const Dev& P, cudaStream_t stream);  // fills ftab, fcoef, fbq, mibref (allocated by the caller)
 // Batched plain steps (kernels.cu): problems of one method advance together,
 // one launch per kernel of the step for all of them.  A launch's CTAs are
 // listed as items (problem, the CTA's index in that problem's own grid, the

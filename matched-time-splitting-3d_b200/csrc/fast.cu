@@ -18,14 +18,15 @@
 // same time as the others.  A step is:
 //
 //   kf_mib  the right-hand side of every MIB row (the explicit MIB sums of
-//           all three directions and the jump terms, one thread per node;
-//           the Convert2Tri row operations of the x blocks, one thread per
-//           block, douglas_adi.cc:1554-1675), written into d at those nodes;
+//           all three directions and the jump terms, one thread per node),
+//           written into d at those nodes;
 //   kf_xw   rho of the regular x lines (and d on the face lines), fused with
 //           their solves: a CTA walks a column of planes for TY lines with
 //           the stencil's planes in a shared-memory ring filled by bulk
 //           copies (see the kernel);
-//   kf_xc   the same for the x lines that cross the interface (side stream);
+//   kf_xc   the same for the x lines that cross the interface, their x
+//           blocks' Convert2Tri row operations first (douglas_adi.cc:
+//           1554-1675) (side stream);
 //   kf_yt   the regular y lines, solved in place on d*, in tiles of NL
 //           neighbouring lines (the same row of NL lines is NL consecutive
 //           doubles) copied into shared memory with cp.async, double-buffered
@@ -455,7 +456,7 @@ __device__ __forceinline__ void load_tab(double* s, const double* g, int w2) {
 __global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, const double* __restrict__ un,
                                               double* __restrict__ d, double E) {
   // every MIB row at once, one thread each (the rows of an x block too:
-  // kf_mib_xblk then applies their block's row operations)
+  // kf_xc applies their block's row operations when it solves the line)
   const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   E = step_e(P, E, 2);
@@ -463,30 +464,6 @@ __global__ void __launch_bounds__(TPB) kf_mib(const __grid_constant__ Dev P, con
   int ix, iy, iz;
   node_xyz(P, m, ix, iy, iz);
   d[m] = rho_mib(P, un, E, m, ix, iy, iz, P.tag[m], P.mibref[k]);
-}
-
-// The Convert2Tri row operations of the x blocks (douglas_adi.cc:1554-1675)
-// on the rows' right-hand sides that kf_mib wrote, one thread per block.
-__global__ void __launch_bounds__(TPB) kf_mib_xblk(const __grid_constant__ Dev P, double* __restrict__ d) {
-  const int t = blockIdx.x * TPB + threadIdx.x;
-  if (t >= P.nblk[0]) return;
-  const MibBlock& b = P.blk[0][t];
-  const int iy = b.line / P.nz, iz = b.line % P.nz;
-  const long long m0 = (long long)P.nx * (iy + (long long)P.ny * iz) + b.L;
-  double r[3] = {0.0, 0.0, 0.0};
-  for (int q = 0; q < b.kind; q++) r[q] = d[m0 + q];
-  if (b.kind == 2) {
-    r[1] -= b.rate[0] * r[0];
-    r[0] -= b.rate[1] * r[1];
-  } else {
-    r[1] -= b.rate[0] * r[0];
-    r[2] -= b.rate[1] * r[0];
-    r[0] -= b.rate[2] * r[2];
-    r[1] -= b.rate[3] * r[2];
-    r[2] -= b.rate[4] * r[1];
-    r[0] -= b.rate[5] * r[1];
-  }
-  for (int q = 0; q < b.kind; q++) d[m0 + q] = r[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -843,7 +820,7 @@ __global__ void __launch_bounds__(32 * CW, 3) kf_xc(const __grid_constant__ Dev 
     x_rho<MX>(P, un, dst, E, iy, iz, buf, lane);
     cf.put_q(qbuf, lane);
     __syncwarp();
-    block_rows<0>(P, buf, qbuf, bfirst, bend, lane, false);  // (the row operations were done by kf_mib)
+    block_rows<0>(P, buf, qbuf, bfirst, bend, lane, true);  // the x blocks' Convert2Tri row operations
     __syncwarp();
     solve_cross<MX>(buf, qbuf, cf, nx, lane);
     __syncwarp();
@@ -1228,9 +1205,8 @@ __global__ void __launch_bounds__(TPB) kf_bq(const __grid_constant__ Dev P, doub
     bq[3 * (long long)k + r] = r < b.kind ? -P.fgam[D][base + (long long)(b.L + r + 1) * s] : 0.0;
 }
 
-// Per MIB node: its block in each direction (-1: none); for the x blocks,
-// the MIB node index of each of their rows.
-__global__ void __launch_bounds__(TPB) kf_mibref(const __grid_constant__ Dev P, int4* ref, int32_t* xbmib) {
+// Per MIB node: its block in each direction (-1: none).
+__global__ void __launch_bounds__(TPB) kf_mibref(const __grid_constant__ Dev P, int4* ref) {
   const int k = blockIdx.x * TPB + threadIdx.x;
   if (k >= P.nmibnode) return;
   const long long m = P.mibnode[k];
@@ -1241,10 +1217,7 @@ __global__ void __launch_bounds__(TPB) kf_mibref(const __grid_constant__ Dev P, 
   int row = 0;
   if (tg & TAG_MIBX) {
     const MibBlock* b = find_block<0>(P, iy * P.nz + iz, ix, row);
-    if (b) {
-      r.x = (int)(b - P.blk[0]);
-      xbmib[3 * r.x + row] = k;
-    }
+    if (b) r.x = (int)(b - P.blk[0]);
   }
   if (tg & TAG_MIBY) {
     const MibBlock* b = find_block<1>(P, ix * P.nz + iz, iy, row);
@@ -1404,8 +1377,7 @@ int build_fast_tables(const Dev& P, cudaStream_t st) {
     launches += 2;
   }
   if (P.nmibnode > 0) {
-    kf_mibref<<<(unsigned)((P.nmibnode + TPB - 1) / TPB), TPB, 0, st>>>(P, const_cast<int4*>(P.mibref),
-                                                                        const_cast<int32_t*>(P.xbmib));
+    kf_mibref<<<(unsigned)((P.nmibnode + TPB - 1) / TPB), TPB, 0, st>>>(P, const_cast<int4*>(P.mibref));
     launches++;
   }
   return launches;
@@ -1440,10 +1412,7 @@ int launch_step_fast(const Dev& P, const StepTimes& T, double* u, double* d, cud
     kf_mib<<<(unsigned)((P.nmibnode + TPB - 1) / TPB), TPB, 0, st>>>(P, u, d, T.e_next);
     launches++;
   }
-  if (P.nblk[0] > 0) {
-    kf_mib_xblk<<<(unsigned)((P.nblk[0] + TPB - 1) / TPB), TPB, 0, st>>>(P, d);
-    launches++;
-  }
+
   pass(0, u, d, nullptr, T.e_next);
   mark(1);
   mark(2);
