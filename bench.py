@@ -212,9 +212,11 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
         s.time = 0.0
         s.initialize()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("batched_steps")  # lets a profiler select the batched launches
     t0 = time.perf_counter()
     M.batch_advance(solvers, steps)
     bat = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
     same = all(s.norms() == r for s, r in zip(solvers, ref))
     # the same mix with its Douglas-ADI problems in the mixed form (FP32
     # segmented line solves inside the multi-problem launches; the other
@@ -240,9 +242,11 @@ def run_batched(count: int, steps: int, seed: int = 0) -> dict:
         s.time = 0.0
         s.initialize()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("batched_steps_mixed")
     t0 = time.perf_counter()
     M.batch_advance(solvers, steps)
     bat_m = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
     same_m = all(s.norms() == r for s, r in zip(solvers, ref_m))
     ratios = [ref_m[i][0] / ref[i][0] for i in adi if ref[i][0] > 0]
     mixed = {
