@@ -84,8 +84,10 @@ typedef struct {
 
 typedef struct mts_problem* mts_handle;
 
-/* Builds the mesh tags, crossing list and MIB weights on the host and
- * uploads the problem to the current CUDA device.  Replaces the setup of
+/* Builds the mesh tags, crossing list and MIB weights (on host threads, or
+ * on the device when params->setup is MTS_SETUP_DEVICE) and places the
+ * problem on the current CUDA device, all of its buffers in one block of the
+ * device's stream-ordered pool.  Replaces the setup of
  *   Mesh::Mesh            src/mesh/mesh.cc:20-70
  *   Intersections ctor    src/spatial/intersection.cc:22-51 (crossings,
  *                         MIB-L1/L2 weights via LU, src/decomposition/lu.cc)
