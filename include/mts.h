@@ -148,12 +148,13 @@ mts_status mts_advance(mts_handle h, int32_t nsteps);
 /* nsteps steps of each of n independent handles, run as one batch: the
  * plain-form handles of one method advance together, one kernel launch per
  * kernel of the step for all of them (each CTA carries its problem and its
- * place in that problem's grid); handles whose lines fill the GPU (256 per
- * SM in every direction) and mixed-precision handles step on their own
- * streams alongside, and the method groups run at once on their own
- * streams.  Each handle's result and
- * time are those of
- * mts_advance(h, nsteps), bit for bit.  Handles must be distinct, on one
+ * place in that problem's grid), and so do the mixed-precision Douglas-ADI
+ * handles whose lines have at most 160 rows, in a group of their own;
+ * handles whose lines fill the GPU (256 per SM in every direction),
+ * fast-form handles and longer-line mixed ones step on their own streams
+ * alongside, and the groups run at once on their own streams.  Each
+ * handle's result and time are those of mts_advance(h, nsteps), bit for
+ * bit.  Handles must be distinct, on one
  * device, with profiling off.  Synchronous.  No counterpart in the
  * reference, which steps one problem per process (helper.h:199-426). */
 mts_status mts_batch_advance(const mts_handle* handles, int32_t n, int32_t nsteps);
