@@ -210,6 +210,17 @@ mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double
  * prints them with 4 digits ("Lmax = ...", "L2   = ..."). */
 mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2);
 
+/* The jumps' error report at the current time: Refresh_Jump's check
+ * (src/spatial/intersection.cc:2294-2490) on the device, one thread per
+ * crossing, the relative error |u_dir - [beta u_d]| / [beta u_d] of the
+ * jump data the solvers are given against the exact flux jump along the
+ * crossing's line (the divisor's sign kept), and Error_Jump's maximum and
+ * root mean square (:4594-4662) added up on the host in its loop order: the
+ * reference's values bit for bit (NaN for Eq_0, whose flux jumps are 0).
+ * The report depends on the geometry and the time only, not on the
+ * solution.  Printed as "Lmax = ...", "L2   = ..." with 4 digits. */
+mts_status mts_jump_errors(mts_handle h, double* lmax, double* l2);
+
 mts_status mts_get_time(mts_handle h, double* t);
 mts_status mts_set_time(mts_handle h, double t);
 

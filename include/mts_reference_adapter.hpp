@@ -180,6 +180,22 @@ class GpuStepper {
     out << std::fixed << std::endl;
   }
 
+  // In place of the reference's report pair
+  //   inter.Refresh_Jump(eq, uh, beta); inter.Error_Jump(out);   (helper.h:233-234)
+  // the jumps' errors at the stepper's time, evaluated on the device
+  // (mts_jump_errors), written in Error_Jump's text (intersection.cc:4656-4661).
+  void Error_Jump(Equation& e, std::ofstream& out) {
+    check_equation(mesh_, e, eq_, bi_, bo_, t_);
+    create();
+    double lmax, l2;
+    check(mts_jump_errors(h_, &lmax, &l2));
+    out << "------------------------ Error of Jumps ------------------------" << std::endl;
+    out << std::setprecision(3) << std::scientific;
+    out << "Lmax = " << lmax << std::endl;
+    out << "L2   = " << l2 << std::endl;
+    out << std::fixed << std::endl;
+  }
+
   mts_handle handle() const { return h_; }
 
  private:

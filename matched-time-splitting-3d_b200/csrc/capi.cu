@@ -83,7 +83,8 @@ struct mts_problem {
   // form; a build that fails part way is done again on the next switch
   bool fast_built = false;
   bool mixed_built = false;
-  // the fictitious points' error report (mts_fp_errors), built on first use
+  // the error reports' tables (mts_fp_errors, mts_jump_errors), built on
+  // first use
   mts_crossing* fp_cr = nullptr;
   int32_t* fp_ci = nullptr;
   int8_t* fp_role = nullptr;
@@ -1233,8 +1234,11 @@ mts_status mts_norms_noalloc(mts_handle h, const double* u_dev, double t, double
   return st;
 }
 
-mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
-  if (!h) return fail(MTS_ERR_ARG, "null handle");
+// The crossing records sorted by (direction, line, position), the order of
+// the report loops of Refresh_Fp / Error_Fp and Refresh_Jump / Error_Jump
+// within a direction, on the device with their handle indices, corner-pair
+// roles and an error buffer of two doubles per record; built on first use.
+static mts_status report_tables(mts_handle h) {
   const int n = (int)h->cross.size();
   if (n > 0 && !h->fp_cr) {
     // the records sorted by (direction, line, position), the order of
@@ -1280,6 +1284,14 @@ mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
     h->fp_role = ro;
     h->fp_err = er;
   }
+  return MTS_OK;
+}
+
+mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  const int n = (int)h->cross.size();
+  mts_status ts = report_tables(h);
+  if (ts != MTS_OK) return ts;
   std::vector<double> err(2 * (size_t)n);
   if (n > 0) {
     h->launches += mts::launch_fp_errors(h->dev, h->fp_cr, h->fp_ci, h->fp_role, n, std::exp(-h->t), h->fp_err,
@@ -1304,6 +1316,35 @@ mts_status mts_fp_errors(mts_handle h, double* lmax, double* l2) {
       if (std::abs(er) > fmax) fmax = std::abs(er);
     }
   if (lmax) *lmax = fmax;
+  if (l2) *l2 = std::sqrt(sum / (double)no);
+  return MTS_OK;
+}
+
+mts_status mts_jump_errors(mts_handle h, double* lmax, double* l2) {
+  if (!h) return fail(MTS_ERR_ARG, "null handle");
+  const int n = (int)h->cross.size();
+  mts_status ts = report_tables(h);
+  if (ts != MTS_OK) return ts;
+  std::vector<double> err((size_t)n);
+  if (n > 0) {
+    h->launches += mts::launch_jump_errors(h->dev, h->fp_cr, h->fp_ci, n, std::exp(-h->t), h->fp_err, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(err.data(), h->fp_err, err.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  mts_status st = sync_status(h);
+  if (st != MTS_OK) return st;
+  // Error_Jump's loops: directions z, y, x, one error per crossing
+  double jmax = 0, sum = 0;
+  long long no = 0;
+  for (int d = 2; d >= 0; d--)
+    for (int i = 0; i < n; i++) {
+      if (h->cross[(size_t)h->fp_perm[(size_t)i]].dir != d) continue;
+      const double e = err[(size_t)i];
+      no += 1;
+      sum += e * e;
+      if (std::abs(e) > jmax) jmax = std::abs(e);
+    }
+  if (lmax) *lmax = jmax;
   if (l2) *l2 = std::sqrt(sum / (double)no);
   return MTS_OK;
 }

@@ -265,6 +265,10 @@ constexpr int kRowPad = 16;  // rows of slack after each staged field (>= chunk 
 // pair, 2 its right (diag.cu).
 int launch_fp_errors(const Dev& P, const mts_crossing* cr, const int32_t* ci, const int8_t* role, int n, double E,
                      double* err, cudaStream_t stream);
+// The jumps' relative errors (Refresh_Jump's jump.err): one per record of
+// the same sorted list into err (diag.cu).
+int launch_jump_errors(const Dev& P, const mts_crossing* cr, const int32_t* ci, int n, double E, double* err,
+                       cudaStream_t stream);
 
 int launch_norms(const Dev& P, double E, const double* u, double* partial, int nblocks,
                  double* out3, cudaStream_t stream);

@@ -60,6 +60,21 @@ __device__ __forceinline__ double step_e(const Dev& P, double given, int k) {
   return P.tsched ? P.tsched[3 * (*P.tstep) + k] : given;
 }
 
+// The exact jumps at crossing q for time factor E: [u] (Equation::Jump_u) and
+// [beta u_x], [beta u_y], [beta u_z] (the Eq's Jump_betau_x/y/z), with the
+// operations of src/equation/eq_0.cc and of the measured problem in their
+// order.
+__device__ __forceinline__ void exact_jumps(const Dev& P, const CrossConst& q, double E, double& ju, double jb[3]) {
+  if (P.eq == 0) {
+    ju = 100.0 - 80.0;
+    for (int d = 0; d < 3; d++) jb[d] = P.bi * 0.0 - P.bo * 0.0;
+  } else {
+    ju = q.R2 * E - q.S * E;
+    const double xyz[3] = {q.x, q.y, q.z};
+    for (int d = 0; d < 3; d++) jb[d] = P.bo * ((2.0 * xyz[d]) * E) - P.bi * (q.D[d] * E);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Line geometry.  Direction D lines are indexed (i1, i2) as in the reference
 // (src/constant.h:83-89): x -> (iy, iz), y -> (ix, iz), z -> (ix, iy); the

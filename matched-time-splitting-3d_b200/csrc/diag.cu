@@ -1,4 +1,6 @@
-// The fictitious points' error report on the device: Refresh_Fp
+// The error reports on the device.
+//
+// Fictitious points: Refresh_Fp
 // (src/spatial/intersection.cc:1841-2281) evaluates, for every crossing, the
 // MIB fictitious values that its weights give from the exact solution and
 // the exact jumps, and their relative error against the exact solution of
@@ -11,6 +13,11 @@
 // in Error_Fp's loop order (directions z, y, x; lines in loop order;
 // crossings by position), so the maximum and the root mean square are the
 // reference's bits too.
+//
+// Jumps: Refresh_Jump (:2294-2490) compares, per crossing, the u_dir it hands
+// the solvers with the exact flux jump along the crossing's line; Error_Jump
+// (:4594-4662) reports their maximum and root mean square, added up on the
+// host in the same order.
 #include <cuda_runtime.h>
 
 #include "../../include/mts.h"
@@ -44,15 +51,9 @@ struct FpLine {
   // Jump_u and Jump_betau along the line at crossing c (Equation::Jump_u,
   // the Eq's Jump_betau_x/y/z)
   __device__ void jumps(int c, double& ju, double& jb) const {
-    if (P.eq == 0) {
-      ju = 100.0 - 80.0;
-      jb = P.bo * 0.0 - P.bi * 0.0;
-      return;
-    }
-    const CrossConst& q = P.cc[c];
-    const double xd = d == 0 ? q.x : d == 1 ? q.y : q.z;
-    ju = q.R2 * E - q.S * E;
-    jb = P.bo * ((2.0 * xd) * E) - P.bi * (q.D[d] * E);
+    double b[3];
+    exact_jumps(P, P.cc[c], E, ju, b);
+    jb = b[d];
   }
 };
 
@@ -119,7 +120,33 @@ __global__ void __launch_bounds__(TPB) k_fp_errors(const __grid_constant__ Dev P
   err[2 * i + 3] = fabs((v2 - rsr) / v2);
 }
 
+// Refresh_Jump's check of the jump data (intersection.cc:2294-2490): per
+// crossing, u_dir = (P^-1)[d][0] [beta u_xi] against the exact [beta u_d]
+// along its line, |u_dir - [beta u_d]| / [beta u_d] (the divisor's sign kept,
+// as there).  Thread i takes record i of the sorted list; ci maps it to the
+// handle's jump constants.
+__global__ void __launch_bounds__(TPB) k_jump_errors(const __grid_constant__ Dev P, const mts_crossing* __restrict__ cr,
+                                                     const int32_t* __restrict__ ci, int n, double E,
+                                                     double* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const CrossConst q = P.cc[ci[i]];
+  double ju, jb[3];
+  exact_jumps(P, q, E, ju, jb);
+  const double bxi = q.p[0] * jb[0] + q.p[1] * jb[1] + q.p[2] * jb[2];
+  const double udir = q.pinv * bxi;
+  const double jd = jb[cr[i].dir];
+  err[i] = fabs(udir - jd) / jd;
+}
+
 }  // namespace
+
+int launch_jump_errors(const Dev& P, const mts_crossing* cr, const int32_t* ci, int n, double E, double* err,
+                       cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_jump_errors<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(P, cr, ci, n, E, err);
+  return 1;
+}
 
 int launch_fp_errors(const Dev& P, const mts_crossing* cr, const int32_t* ci, const int8_t* role, int n, double E,
                      double* err, cudaStream_t st) {

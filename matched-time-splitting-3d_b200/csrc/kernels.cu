@@ -910,14 +910,7 @@ __device__ __forceinline__ void k_jumps_body(const Dev& P, unsigned cta_, unsign
   E = step_e(P, E, 2);
   const CrossConst q = P.cc[c];
   double ju, jb[3];
-  if (P.eq == 0) {
-    ju = 100.0 - 80.0;
-    for (int d = 0; d < 3; d++) jb[d] = P.bi * 0.0 - P.bo * 0.0;
-  } else {
-    ju = q.R2 * E - q.S * E;
-    const double xyz[3] = {q.x, q.y, q.z};
-    for (int d = 0; d < 3; d++) jb[d] = P.bo * ((2.0 * xyz[d]) * E) - P.bi * (q.D[d] * E);
-  }
+  exact_jumps(P, q, E, ju, jb);
   double bxi = q.p[0] * jb[0] + q.p[1] * jb[1] + q.p[2] * jb[2];
   P.jv[c] = make_double2(ju, q.pinv * bxi);
 }

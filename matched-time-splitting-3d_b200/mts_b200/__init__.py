@@ -296,6 +296,15 @@ class Solver:
         check(self._L.mts_fp_errors(self._h, ctypes.byref(a), ctypes.byref(b)), "mts_fp_errors")
         return a.value, b.value
 
+    def jump_errors(self):
+        """The jumps' error report at the current time (mts_jump_errors:
+        Refresh_Jump's check + Error_Jump on the device): (L-infinity, root
+        mean square) of the relative errors of the jump data the solvers are
+        given against the exact flux jumps."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(self._L.mts_jump_errors(self._h, ctypes.byref(a), ctypes.byref(b)), "mts_jump_errors")
+        return a.value, b.value
+
     def stream(self) -> int:
         v = ctypes.c_void_p()
         check(self._L.mts_get_stream(self._h, ctypes.byref(v)), "mts_get_stream")

@@ -45,6 +45,7 @@ EXPORTS = [
     "mts_norms",
     "mts_norms_noalloc",
     "mts_fp_errors",
+    "mts_jump_errors",
     "mts_get_time",
     "mts_set_time",
     "mts_synchronize",
@@ -170,6 +171,7 @@ def load(build_if_missing: bool = True):
             "mts_norms": [H, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_norms_noalloc": [H, vp, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double), vp],
             "mts_fp_errors": [H, P(ctypes.c_double), P(ctypes.c_double)],
+            "mts_jump_errors": [H, P(ctypes.c_double), P(ctypes.c_double)],
             "mts_get_time": [H, P(ctypes.c_double)],
             "mts_set_time": [H, ctypes.c_double],
             "mts_synchronize": [H],

@@ -174,6 +174,7 @@ struct Args {
   string report;     // --report F: the stepper's own Error() text at the end
   bool write_txt = false;  // --write-txt: the reference's Write_txt files (Eq_0..Eq_7) at the end
   string fp_errors;  // --fp-errors F: Refresh_Fp + Error_Fp at the end (values in binary, then the text)
+  string jump_errors;  // --jump-errors F: Refresh_Jump + Error_Jump at the end (the same layout)
   bool gpu = false;  // --gpu: mts::GpuStepper in place of the reference's stepper
   int beta_plugin = -1;  // --beta-plugin 1: the reference's Beta_1 instead of the piecewise-constant beta
 };
@@ -184,7 +185,8 @@ struct Args {
           "        --surface ellipsoid a b c r [cx cy cz] | torus R r\n"
           "        --beta bi bo [--beta-plugin 1] --eq 0|3|8 --method adi|lod-ie|lod-cn|ts --mib 1|2\n"
           "        --dt DT [--t0 T0] (--steps K | --t-end T)\n"
-          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F] [--fp-errors F] [--write-txt]\n"
+          "        [--dump-u F] [--dump-u0 F] [--dump-tags F] [--dump-mib F] [--report F] [--fp-errors F] [--jump-errors F]\n"
+          "        [--write-txt]\n"
 #ifdef MTS_DROPIN
           "        [--gpu]\n"
 #endif
@@ -258,6 +260,9 @@ Args parse(int argc, char** argv) {
     } else if (k == "--fp-errors") {
       need(1);
       a.fp_errors = argv[++i];
+    } else if (k == "--jump-errors") {
+      need(1);
+      a.jump_errors = argv[++i];
 #ifdef MTS_DROPIN
     } else if (k == "--gpu") {
       a.gpu = true;
@@ -485,6 +490,10 @@ int main(int argc, char** argv) {
         ofstream o(a.fp_errors + ".gpu");
         st.Error_Fp(*make_eq(a, t_now, beta), o);
       }
+      if (!a.jump_errors.empty()) {
+        ofstream o(a.jump_errors + ".gpu");
+        st.Error_Jump(*make_eq(a, t_now, beta), o);
+      }
     } catch (const std::exception& e) {
       fprintf(stderr, "mts_dropin: %s\n", e.what());
       return 3;
@@ -545,6 +554,38 @@ int main(int argc, char** argv) {
     fclose(f);
     ofstream txt(a.fp_errors, ios::app);
     inter.Error_Fp(txt);
+  }
+  if (!a.jump_errors.empty()) {
+    // The jumps' errors at the final time (helper.h:233-234): Refresh_Jump,
+    // then Error_Jump's maximum and root mean square recomputed here in its
+    // loop order (intersection.cc:4594-4662), followed by its own text.  In
+    // the noaux build Refresh_Jump's eta / tau estimates are 0, which
+    // Error_Jump does not read.
+    inter.Refresh_Jump(*make_eq(a, t_now, beta), uh, beta);
+    double jmax = 0, jsum = 0;
+    long long jno = 0;
+    auto add = [&](Intersection_Data& d) {
+      jno += 1;
+      jsum += d.jump.err * d.jump.err;
+      if (fabs(d.jump.err) > jmax) jmax = fabs(d.jump.err);
+    };
+    for (int ix = 1; ix < nx - 1; ix++)
+      for (int iy = 1; iy < ny - 1; iy++)
+        for (auto& d : inter.ifpz[ix][iy])
+          if (d.ID != 0) add(d);
+    for (int ix = 1; ix < nx - 1; ix++)
+      for (int iz = 1; iz < nz - 1; iz++)
+        for (auto& d : inter.ifpy[ix][iz])
+          if (d.ID != 0) add(d);
+    for (int iy = 1; iy < ny - 1; iy++)
+      for (int iz = 1; iz < nz - 1; iz++)
+        for (auto& d : inter.ifpx[iy][iz])
+          if (d.ID != 0) add(d);
+    FILE* f = fopen(a.jump_errors.c_str(), "w");
+    fprintf(f, "%.17g %.17g %.17g %lld\n", jmax, sqrt(jsum / jno), jsum, jno);
+    fclose(f);
+    ofstream txt(a.jump_errors, ios::app);
+    inter.Error_Jump(txt);
   }
 
   printf(

@@ -1,8 +1,10 @@
 """Generates tests/golden/fp_errors.json: the reference's fictitious-point
 error report (Refresh_Fp then Error_Fp, src/spatial/intersection.cc:1841-2281,
-4667-4771) at the end of short runs, from the reference's own code
-(oracle/_ref/mts_ref_noaux --fp-errors, built by oracle/Makefile; the noaux
-build leaves Refresh_Fp and the solution unchanged).  Needs the reference
+4667-4771) and its jump error report (Refresh_Jump then Error_Jump,
+:2294-2490, 4594-4662; under the key "jump") at the end of short runs, from
+the reference's own code (oracle/_ref/mts_ref_noaux --fp-errors
+--jump-errors, built by oracle/Makefile; the noaux build leaves Refresh_Fp,
+the jump errors and the solution unchanged).  Needs the reference
 tree; the GPU box only reads the committed JSON.
 
     make -C oracle REF=<reference checkout> && python tests/golden/make_fp_golden.py
@@ -54,20 +56,24 @@ def main():
     for name, prob in cases():
         with tempfile.TemporaryDirectory() as td:
             f = os.path.join(td, "fp.txt")
-            cp = subprocess.run([O.REF_BIN_NOAUX, *prob.ref_args(), "--fp-errors", f], capture_output=True, text=True,
-                                timeout=600)
+            fj = os.path.join(td, "jump.txt")
+            cp = subprocess.run([O.REF_BIN_NOAUX, *prob.ref_args(), "--fp-errors", f, "--jump-errors", fj],
+                                capture_output=True, text=True, timeout=600)
             if cp.returncode != 0:
                 raise RuntimeError(cp.stderr[-400:])
             info = json.loads([ln for ln in cp.stdout.splitlines() if ln.startswith("{")][-1])
             lines = open(f).read().splitlines()
+            jlines = open(fj).read().splitlines()
         lmax, l2, s, no = lines[0].split()
+        jmax, jl2, js, jno = jlines[0].split()
         d = dict(prob.__dict__)
         d["n"] = list(prob.n)
         d["domain"] = list(prob.domain)
         d["surface_params"] = list(prob.surface_params)
         out[name] = {"problem": d, "t": info["t"], "lmax": lmax, "l2": l2, "sum": s, "count": int(no),
-                     "text": "\n".join(lines[1:])}
-        print(name, lmax, l2, no)
+                     "text": "\n".join(lines[1:]),
+                     "jump": {"lmax": jmax, "l2": jl2, "sum": js, "count": int(jno), "text": "\n".join(jlines[1:])}}
+        print(name, lmax, l2, no, "jumps:", jmax, jl2, jno)
     with open(os.path.join(HERE, "fp_errors.json"), "w") as fo:
         json.dump(out, fo, indent=1, sort_keys=True)
 

@@ -78,19 +78,22 @@ def test_dropin_gpu_equals_reference_bitwise(name, prob, tmp_path):
 @pytest.mark.gpu
 @needs_dropin
 @pytest.mark.parametrize("mib", [1, 2])
-def test_dropin_fp_error_report(mib, tmp_path):
-    """The stepper's Error_Fp (the device's Refresh_Fp + Error_Fp) writes the
-    same report as the reference's Intersections::Error_Fp in the same run."""
+def test_dropin_error_reports(mib, tmp_path):
+    """The stepper's Error_Fp and Error_Jump (the device's Refresh_Fp +
+    Error_Fp, Refresh_Jump's check + Error_Jump) write the same reports as
+    the reference's Intersections::Error_Fp and Error_Jump in the same run."""
     prob = O.Problem(n=(26, 30, 28), surface="ellipsoid", surface_params=(0.61, 0.52, 0.43, 1.0, 0.05, -0.03, 0.02),
                      beta_in=1.0, beta_out=100.0, method="adi", mib=mib, dt=1.0 / 16, steps=3)
     f = tmp_path / "fp.txt"
-    cp = subprocess.run([O.REF_BIN_DROPIN, *prob.ref_args(), "--gpu", "--fp-errors", str(f)], capture_output=True,
-                        text=True, timeout=300)
+    fj = tmp_path / "jump.txt"
+    cp = subprocess.run([O.REF_BIN_DROPIN, *prob.ref_args(), "--gpu", "--fp-errors", str(f), "--jump-errors",
+                         str(fj)], capture_output=True, text=True, timeout=300)
     assert cp.returncode == 0, cp.stderr
-    ref_text = "\n".join(f.read_text().splitlines()[1:])
-    gpu_text = (tmp_path / "fp.txt.gpu").read_text()
-    assert "Error of FPs" in ref_text and "inf" not in ref_text and "nan" not in ref_text
-    assert gpu_text.strip() == ref_text.strip()
+    for path, title in ((f, "Error of FPs"), (fj, "Error of Jumps")):
+        ref_text = "\n".join(path.read_text().splitlines()[1:])
+        gpu_text = (tmp_path / (path.name + ".gpu")).read_text()
+        assert title in ref_text and "inf" not in ref_text and "nan" not in ref_text
+        assert gpu_text.strip() == ref_text.strip()
 
 
 @pytest.mark.gpu
