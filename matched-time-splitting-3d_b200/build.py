@@ -6,7 +6,8 @@ Host code (setup, C ABI) and device code are compiled without floating-point
 contraction (-fmad=false for the device, -ffp-contract=off for the host): the
 plain FP64 path must round every product and sum on its own, as the reference
 CPU build does.  The fast FP64 form (fast.cu), whose results are only required
-to match the reference to rounding, is compiled with fused multiply-adds.
+to match the reference to rounding, and the mixed-precision form (mixed.cu),
+held to an accuracy bound, are compiled with fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -25,7 +26,7 @@ HEADERS = ["setup.h", "device.h", "device_common.cuh"]
 OBJ_DIR = os.path.join(HERE, "build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # device code of these sources may contract a*b+c into one fused multiply-add
-FMA_SOURCES = {"fast.cu"}
+FMA_SOURCES = {"fast.cu", "mixed.cu"}
 
 
 def nvcc() -> str:
