@@ -10,6 +10,11 @@
  * returns an mts_status; no function exits or throws.  Functions on one
  * handle are not thread-safe; distinct handles are independent (one CUDA
  * stream each).
+ *
+ * A handle lives on the CUDA device that was current when it was created.
+ * Call the functions that take it with that device current (the usual one
+ * process per GPU does so by construction); a batch takes handles of one
+ * device.
  */
 #ifndef MTS_H
 #define MTS_H
